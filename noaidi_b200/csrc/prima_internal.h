@@ -1,0 +1,115 @@
+// Internal declarations shared by the translation units of libprima_cuda.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "prima_cuda.h"
+
+namespace prima {
+
+// ---- errors -----------------------------------------------------------------
+void set_error(const std::string &msg);
+void clear_error();
+
+struct Error {
+  int32_t code;
+  std::string msg;
+};
+
+#define PRIMA_CUDA_TRY(expr)                                                            \
+  do {                                                                                  \
+    cudaError_t _e = (expr);                                                            \
+    if (_e != cudaSuccess) {                                                            \
+      ::prima::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));           \
+      return _e == cudaErrorMemoryAllocation ? PRIMA_ERR_OUT_OF_MEMORY : PRIMA_ERR_CUDA; \
+    }                                                                                   \
+  } while (0)
+
+// ---- device buffers ---------------------------------------------------------
+struct DeviceBuffer {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer &) = delete;
+  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+  ~DeviceBuffer();
+  int32_t reserve(size_t b);  // grows, never shrinks; contents not preserved
+  void release();
+};
+
+// A seam vector: n elements of the context's storage precision.
+struct Vec {
+  int64_t n = 0;
+  DeviceBuffer buf;
+};
+
+// A seam matrix: CSR with values in the context's precision.
+struct Mat {
+  int32_t rows = 0, cols = 0;
+  int64_t nnz = 0;
+  DeviceBuffer row_ptr, col_idx, vals;
+  int32_t lanes = 1;  // SpMV variant picked by the autotuner (1 = thread per row)
+};
+
+struct Ctx {
+  int32_t device = 0;
+  int32_t bits = 64;
+  bool closed = false;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  std::string device_name;
+  int64_t next_id = 1;
+  std::unordered_map<int64_t, std::unique_ptr<Vec>> vecs;
+  std::unordered_map<int64_t, std::unique_ptr<Mat>> mats;
+  DeviceBuffer scratch;        // reduction partials and staging for the seam ops
+  double *host_scalar = nullptr;  // pinned: reduction results
+  int32_t *cancel_mapped = nullptr;  // pinned + mapped: cancel flag seen by the device
+  int32_t *cancel_mapped_dev = nullptr;
+  DeviceBuffer solver_arena;   // buffers of the coarse solvers, reused across solves
+};
+
+// Registry lookup (thread-safe); returns nullptr and sets the error on failure.
+Ctx *lookup_ctx(prima_handle h, int32_t *code);
+
+// ---- host-side problem preparation (prima_host.cpp) -----------------------
+struct Csr {
+  int32_t rows = 0, cols = 0;
+  std::vector<int32_t> row_ptr;
+  std::vector<int32_t> col_idx;
+  std::vector<double> vals;
+  int64_t nnz() const { return rows ? row_ptr[rows] : 0; }
+};
+
+// The equilibrated problem and the diagonals that undo it (Scaling.scala:32-61).
+struct ScaledLp {
+  int32_t n = 0, m = 0, neq = 0;
+  Csr K, Kt;  // scaled matrix and its materialised transpose
+  std::vector<double> c, q, l, u;
+  std::vector<double> row_scale, col_scale;
+  double scaled_spectral_bound = 0.0;  // opening step: 1 / bound
+  double orig_spectral_bound = 0.0;    // certificate normalisation
+  double rhs_norm = 0.0, obj_norm = 0.0;  // norms of the original q and c
+  double scaled_c_norm = 0.0, scaled_q_norm = 0.0;
+};
+
+// LpProblem.apply's requirements (LpProblem.scala:62-104) plus CSR sanity.
+int32_t validate_lp(const prima_lp *lp);
+// PdhgParams / ScalingParams requirements (PdhgParams.scala:55-79).
+int32_t validate_params(const prima_params *p);
+// Scaling.apply (Scaling.scala:77-155) + transpose + norms, on the host.
+void prepare_scaled(const prima_lp *lp, const prima_params *p, ScaledLp *out);
+void csr_transpose(const Csr &a, Csr *t);
+double csr_norm_inf(const Csr &a);
+double spectral_norm_bound(const Csr &a, const Csr &at);
+
+// ---- SpMV helpers for the seam (prima_ops.cu) ------------------------------
+int32_t seam_spmv(Ctx *ctx, const Mat *a, const void *x, void *out);
+
+}  // namespace prima

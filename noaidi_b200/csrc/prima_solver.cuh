@@ -1,0 +1,134 @@
+// Fused, persistent restarted-PDHG solver (device side).
+//
+// One cooperative launch runs a whole solve: the iteration, the adaptive
+// step-size rule, the checkpoint evaluation (FP64 KKT + Farkas certificates),
+// restarts and termination -- Pdhg.Solve (core/Pdhg.scala:123-534) with the
+// host loop moved onto the GPU.  Blocks of a team step through phases
+// separated by team barriers; at each barrier the LAST block to arrive reduces
+// the phase's per-block partial sums (a fixed tree: deterministic) and runs
+// the scalar tail of the algorithm, then publishes the next phase in a
+// Control record every block reads.  No host round trip per iteration.
+//
+// Phases and what each fuses (rows r of K over m, columns j over n):
+//   INIT  kx = K x0, kty = K'y0, restart points, zero sums, KKT of the start
+//   A     [pending commit: kty = K'y_new, sumX/sumKtY += w*(x, kty)]
+//         x' = clamp(x - tau(c - kty)), xbar = 2x' - x, sum (x'-x)^2
+//   B     [pending commit: sumY/sumKx += w*(y, kx)]
+//         kxbar = K xbar, y' = proj(y + sigma(q - kxbar)), kx' = (kxbar+kx)/2,
+//         sum (y'-y)^2, sum (y'-y).(kxbar-kx)/2
+//   F     flush pending commit, optional fresh kx = K x, FP64 KKT of the
+//         current point and of the running average, certificate terms
+//   R     restart: optionally adopt the average, |x - xr|, |y - yr|, reset
+//   W     write the solution in the caller's units (FP64)
+// A/B form one step-size trial; an accepted trial commits by flipping the
+// double-buffered x, y, kx (no copies) and leaves the K'y product and the
+// running-sum updates pending for the next A/B (or F) pass, which reads the
+// same vectors anyway.
+//
+// Element arithmetic is exactly the reference kernel expressions in the
+// storage type T (double: ScalaKernels; float: Float32Kernels), built with
+// --fmad=false; every row of K and K' is summed in index order from zero, so
+// a double-precision team reproduces the reference's SpMV bit for bit.
+// Reductions are in double, in a fixed tree order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace prima {
+namespace dev {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxQ = 17;
+
+enum : int { PH_INIT = 0, PH_A = 1, PH_B = 2, PH_F = 3, PH_R = 4, PH_W = 5, PH_DONE = 6 };
+enum : int { F_FIXPOINT = 0, F_CHECKPOINT = 1, F_ITERLIMIT = 2 };
+
+// Reduction slots.  Trial: A writes DX, B writes DY and INTER.  Evaluation:
+// current-point terms, then average-point terms.  Restart: DXR, DYR.
+enum : int { Q_DX = 0, Q_DY = 1, Q_INTER = 2 };
+enum : int {
+  Q_PSQ = 0,   // primal residual^2           (rows)
+  Q_QY,        // q'y                          (rows)
+  Q_YSQ,       // |y|^2                        (rows, primal certificate)
+  Q_CONE,      // dual-cone violation^2        (rows, primal certificate)
+  Q_ROWSQ,     // Kx row violation^2           (rows, dual certificate)
+  Q_CX,        // c'x                          (cols)
+  Q_DTERM,     // bound terms of the dual obj  (cols)
+  Q_DSQ,       // dual residual^2              (cols)
+  Q_PVAL,      // bound terms of the primal certificate value (cols)
+  Q_PRSQ,      // unabsorbed reduced cost^2 of the primal certificate (cols)
+  Q_XSQ,       // |x|^2                        (cols, dual certificate)
+  Q_BSQ,       // bound violation^2            (cols, dual certificate)
+  Q_A_PSQ,     // the same KKT terms for the running average
+  Q_A_QY,
+  Q_A_CX,
+  Q_A_DTERM,
+  Q_A_DSQ,
+  Q_EVAL_N
+};
+enum : int { Q_DXR = 0, Q_DYR = 1 };
+static_assert(Q_EVAL_N == kMaxQ, "slot count");
+
+struct Kkt {
+  double pres, dres, pobj, dobj;
+};
+
+struct Params {
+  double eps_abs, eps_rel, rhs_norm, obj_norm;
+  int32_t max_iterations, eval_freq;
+  double time_limit_ms, setup_ms;
+  double infeas_tol, r_suff, r_nec, r_art, smoothing;
+  double matrix_norm;  // spectral bound of the ORIGINAL matrix (certificates)
+  double offset;
+};
+
+// Published by the deciding block at every barrier.
+struct Control {
+  int32_t phase, f_mode, f_avg, r_avg;
+  int32_t w_avg, pend, xc, yc;
+  int32_t kxc, status, iteration, restarts;
+  int32_t last_restart_it, trials, error, pad;
+  int64_t total_trials;
+  uint64_t t0;
+  double step, weight, weight_sum, pend_w;
+  double inv_w, tau, sigma, error_at_restart;
+  double last_candidate, pad2;
+  Kkt current, average, final_kkt;
+};
+
+struct Sync {
+  unsigned int count;
+  unsigned int gen;
+  int32_t abort;
+  int32_t pad;
+};
+
+template <typename T>
+struct Args {
+  int32_t n, m, neq, pad;
+  // equilibrated matrix and its transpose, CSR
+  const int32_t *kp, *kci;
+  const T *kv;
+  const int32_t *tp, *tci;
+  const T *tv;
+  // equilibrated data in the storage type
+  const T *c, *q, *l, *u;
+  // original data and the diagonals (FP64)
+  const double *c0, *q0, *l0, *u0, *cs, *rs;
+  // iterate state; x, y, kx are double-buffered
+  T *x[2], *y[2], *kx[2];
+  T *xbar, *kty, *sx, *sy, *skx, *skty, *xr, *yr;
+  // solution in the caller's units
+  double *xo, *yo, *rco;
+  double *partials;  // [kMaxQ][max_blocks]
+  int32_t max_blocks, pad2;
+  Control *ctl;
+  Sync *sync;
+  const volatile int32_t *cancel;
+  Params P;
+};
+
+}  // namespace dev
+}  // namespace prima

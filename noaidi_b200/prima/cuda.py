@@ -1,0 +1,407 @@
+"""ctypes binding of ``libprima_cuda.so`` (declared in ``include/prima_cuda.h``).
+
+* :class:`CudaKernels` -- the ``Kernels`` seam (``Kernels.scala:42-125``) on a
+  B200: the eight numeric operations over device-resident vectors.
+* :func:`solve` -- ``Pdhg.solveWith`` (``Pdhg.scala:48-55``) with the whole
+  iteration on the device (one persistent launch).
+* :func:`mixed_solve` -- ``MixedPrecision.solve`` (``MixedPrecision.scala:104-199``)
+  with both passes on the device.
+* :func:`solve_batch` -- ``PrimaZio.solveAll``'s shape in one launch.
+
+There is no CPU fallback: if the library is missing or no sm_100 device is
+present these raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import threading
+from typing import Optional, Sequence
+
+import numpy as np
+
+from .model import LpProblem, SparseMatrix
+from .types import (KktError, LpSolution, MixedPrecisionParams, MixedPrecisionResult, PdhgParams, SolveStatus,
+                    WarmStart)
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "libprima_cuda.so")
+
+OK, ERR_INVALID_ARGUMENT, ERR_OUT_OF_MEMORY, ERR_CUDA, ERR_TIMEOUT, ERR_CLOSED, ERR_NO_DEVICE = range(7)
+MIXED_TWO_PASS, MIXED_REFINEMENT = 0, 1
+
+
+class PrimaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class Capabilities(C.Structure):
+    _fields_ = [("name", C.c_char * 64), ("device", C.c_char * 128), ("supports_float64", C.c_int32),
+                ("precision_bits", C.c_int32)]
+
+
+class CLp(C.Structure):
+    _fields_ = [("num_variables", C.c_int32), ("num_constraints", C.c_int32), ("num_equalities", C.c_int32),
+                ("pad", C.c_int32), ("row_ptr", C.POINTER(C.c_int32)), ("col_idx", C.POINTER(C.c_int32)),
+                ("values", C.POINTER(C.c_double)), ("objective", C.POINTER(C.c_double)),
+                ("rhs", C.POINTER(C.c_double)), ("lower", C.POINTER(C.c_double)),
+                ("upper", C.POINTER(C.c_double)), ("objective_offset", C.c_double)]
+
+
+class CParams(C.Structure):
+    _fields_ = [("eps_abs", C.c_double), ("eps_rel", C.c_double), ("max_iterations", C.c_int32),
+                ("evaluation_frequency", C.c_int32), ("time_limit_ms", C.c_double),
+                ("ruiz_iterations", C.c_int32), ("apply_pock_chambolle", C.c_int32),
+                ("pock_chambolle_alpha", C.c_double), ("infeasibility_tolerance", C.c_double),
+                ("restart_sufficient_reduction", C.c_double), ("restart_necessary_reduction", C.c_double),
+                ("restart_artificial_fraction", C.c_double), ("primal_weight_smoothing", C.c_double)]
+
+
+class CWarm(C.Structure):
+    _fields_ = [("primal", C.POINTER(C.c_double)), ("dual", C.POINTER(C.c_double)), ("step_size", C.c_double),
+                ("primal_weight", C.c_double)]
+
+
+class CInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("restarts", C.c_int32),
+                ("device_error", C.c_int32), ("solve_ms", C.c_int64), ("objective", C.c_double),
+                ("dual_objective", C.c_double), ("primal_residual", C.c_double), ("dual_residual", C.c_double),
+                ("final_step_size", C.c_double), ("final_primal_weight", C.c_double), ("device_ms", C.c_double),
+                ("setup_ms", C.c_double), ("trials", C.c_int64)]
+
+
+class CMixedParams(C.Structure):
+    _fields_ = [("reduced_tolerance", C.c_double), ("reduced_max_iterations", C.c_int32),
+                ("always_refine", C.c_int32), ("reduced_time_share", C.c_double), ("scheme", C.c_int32),
+                ("max_refinements", C.c_int32), ("refinement_growth", C.c_double)]
+
+
+class CMixedInfo(C.Structure):
+    _fields_ = [("reduced_iterations", C.c_int32), ("reduced_restarts", C.c_int32), ("reduced_ms", C.c_int64),
+                ("refinement_iterations", C.c_int32), ("refined", C.c_int32), ("refinement_ms", C.c_int64),
+                ("refinement_rounds", C.c_int32), ("pad", C.c_int32)]
+
+
+# Every exported symbol with its ctypes signature; the ABI test checks this
+# list against include/prima_cuda.h.
+_H = C.c_int64
+_HP = C.POINTER(C.c_int64)
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int32)
+SIGNATURES = {
+    "prima_last_error": (C.c_char_p, []),
+    "prima_open": (C.c_int32, [C.c_int32, C.c_int32, _HP]),
+    "prima_close": (C.c_int32, [_H]),
+    "prima_capabilities_get": (C.c_int32, [_H, C.POINTER(Capabilities)]),
+    "prima_vec_alloc": (C.c_int32, [_H, C.c_int64, _HP]),
+    "prima_vec_upload": (C.c_int32, [_H, _DP, C.c_int64, _HP]),
+    "prima_vec_download": (C.c_int32, [_H, _H, _DP, C.c_int64]),
+    "prima_vec_length": (C.c_int32, [_H, _H, C.POINTER(C.c_int64)]),
+    "prima_vec_free": (C.c_int32, [_H, _H]),
+    "prima_mat_upload_csr": (C.c_int32, [_H, C.c_int32, C.c_int32, _IP, _IP, _DP, _HP]),
+    "prima_spmv": (C.c_int32, [_H, _H, _H, _H]),
+    "prima_axpby": (C.c_int32, [_H, C.c_double, _H, C.c_double, _H, _H]),
+    "prima_scale": (C.c_int32, [_H, C.c_double, _H, _H]),
+    "prima_copy": (C.c_int32, [_H, _H, _H]),
+    "prima_dot": (C.c_int32, [_H, _H, _H, _DP]),
+    "prima_squared_norm": (C.c_int32, [_H, _H, _DP]),
+    "prima_primal_step": (C.c_int32, [_H, _H, _H, _H, _H, _H, C.c_double, _H]),
+    "prima_dual_step": (C.c_int32, [_H, _H, _H, _H, C.c_double, C.c_int32, _H]),
+    "prima_params_default": (None, [C.POINTER(CParams)]),
+    "prima_mixed_params_default": (None, [C.POINTER(CMixedParams)]),
+    "prima_pdhg_solve": (C.c_int32, [_H, C.POINTER(CLp), C.POINTER(CParams), C.POINTER(CWarm), _IP, _DP, _DP,
+                                     _DP, C.POINTER(CInfo)]),
+    "prima_mixed_solve": (C.c_int32, [_H, C.POINTER(CLp), C.POINTER(CParams), C.POINTER(CMixedParams), _IP,
+                                      _DP, _DP, _DP, C.POINTER(CInfo), C.POINTER(CMixedInfo)]),
+    "prima_pdhg_solve_batch": (C.c_int32, [_H, C.c_int32, C.POINTER(CLp), C.POINTER(CParams), _IP,
+                                           C.POINTER(_DP), C.POINTER(_DP), C.POINTER(_DP), C.POINTER(CInfo)]),
+}
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def library():
+    """Load ``libprima_cuda.so`` (never a fallback: a missing library raises)."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise PrimaError(ERR_NO_DEVICE, f"{LIB_PATH} is missing; build it with `python -m noaidi_b200.build`")
+            lib = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def _check(code: int) -> None:
+    if code != OK:
+        msg = library().prima_last_error().decode()
+        if code == ERR_INVALID_ARGUMENT:
+            raise ValueError(msg)
+        raise PrimaError(code, msg)
+
+
+def _dp(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_DP)
+
+
+def _ip(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_IP)
+
+
+def to_c_params(p: PdhgParams) -> CParams:
+    return CParams(p.eps_abs, p.eps_rel, p.max_iterations, p.evaluation_frequency,
+                   -1.0 if p.time_limit_millis is None else float(p.time_limit_millis),
+                   p.scaling.ruiz_iterations, int(p.scaling.apply_pock_chambolle), p.scaling.pock_chambolle_alpha,
+                   p.infeasibility_tolerance, p.restart_sufficient_reduction, p.restart_necessary_reduction,
+                   p.restart_artificial_fraction, p.primal_weight_smoothing)
+
+
+class _LpView:
+    """A prima_lp over a problem's arrays (kept alive by this object)."""
+
+    def __init__(self, problem: LpProblem):
+        K = problem.constraint_matrix
+        self._keep = (np.ascontiguousarray(K.row_ptr, np.int32), np.ascontiguousarray(K.col_indices, np.int32),
+                      np.ascontiguousarray(K.values, np.float64), np.ascontiguousarray(problem.objective),
+                      np.ascontiguousarray(problem.rhs), np.ascontiguousarray(problem.variable_lower),
+                      np.ascontiguousarray(problem.variable_upper))
+        rp, ci, v, c, q, lo, hi = self._keep
+        self.c = CLp(problem.num_variables, problem.num_constraints, problem.num_equalities, 0, _ip(rp), _ip(ci),
+                     _dp(v), _dp(c), _dp(q), _dp(lo), _dp(hi), problem.objective_offset)
+
+
+class Context:
+    """An open ``libprima_cuda`` context (a ``Kernels`` instance's device state)."""
+
+    def __init__(self, device: int = 0, precision: int = 64):
+        self.lib = library()
+        h = C.c_int64()
+        _check(self.lib.prima_open(device, precision, C.byref(h)))
+        self.handle = h.value
+        self.precision = precision
+        self._closed = False
+
+    def close(self) -> None:
+        if not self._closed:
+            _check(self.lib.prima_close(self.handle))
+            self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CudaKernels:
+    """``Kernels`` on a B200 (``Kernels.scala:42-125``).  ``precision=64`` has
+    ScalaKernels semantics, ``precision=32`` Float32Kernels semantics.
+    Vectors and matrices are integer handles owned by the context."""
+
+    def __init__(self, device: int = 0, precision: int = 64):
+        self.ctx = Context(device, precision)
+        self.lib = self.ctx.lib
+        self.h = self.ctx.handle
+
+    # capabilities ------------------------------------------------------------
+    @property
+    def capabilities(self):
+        caps = Capabilities()
+        _check(self.lib.prima_capabilities_get(self.h, C.byref(caps)))
+        return _Caps(caps.name.decode(), caps.device.decode(), bool(caps.supports_float64))
+
+    # memory --------------------------------------------------------------------
+    def allocate(self, n: int) -> int:
+        v = C.c_int64()
+        _check(self.lib.prima_vec_alloc(self.h, n, C.byref(v)))
+        return v.value
+
+    def upload(self, data) -> int:
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        v = C.c_int64()
+        _check(self.lib.prima_vec_upload(self.h, _dp(a), a.shape[0], C.byref(v)))
+        return v.value
+
+    def download(self, v: int, into: np.ndarray) -> None:
+        if into.dtype != np.float64 or not into.flags.c_contiguous:
+            raise ValueError("download target must be a contiguous float64 array")
+        _check(self.lib.prima_vec_download(self.h, v, _dp(into), into.shape[0]))
+
+    def upload_matrix(self, m: SparseMatrix) -> int:
+        h = C.c_int64()
+        rp = np.ascontiguousarray(m.row_ptr, np.int32)
+        ci = np.ascontiguousarray(m.col_indices, np.int32)
+        vv = np.ascontiguousarray(m.values, np.float64)
+        _check(self.lib.prima_mat_upload_csr(self.h, m.rows, m.cols, _ip(rp), _ip(ci), _dp(vv), C.byref(h)))
+        return h.value
+
+    def length(self, v: int) -> int:
+        n = C.c_int64()
+        _check(self.lib.prima_vec_length(self.h, v, C.byref(n)))
+        return n.value
+
+    def close(self) -> None:
+        self.ctx.close()
+
+    # numerics ------------------------------------------------------------------
+    def spmv(self, a: int, x: int, out: int) -> None:
+        _check(self.lib.prima_spmv(self.h, a, x, out))
+
+    def axpby(self, alpha: float, x: int, beta: float, y: int, out: int) -> None:
+        _check(self.lib.prima_axpby(self.h, alpha, x, beta, y, out))
+
+    def scale(self, alpha: float, x: int, out: int) -> None:
+        _check(self.lib.prima_scale(self.h, alpha, x, out))
+
+    def copy(self, src: int, dst: int) -> None:
+        _check(self.lib.prima_copy(self.h, src, dst))
+
+    def dot(self, x: int, y: int) -> float:
+        out = C.c_double()
+        _check(self.lib.prima_dot(self.h, x, y, C.byref(out)))
+        return out.value
+
+    def squared_norm(self, x: int) -> float:
+        out = C.c_double()
+        _check(self.lib.prima_squared_norm(self.h, x, C.byref(out)))
+        return out.value
+
+    def primal_step(self, x: int, kty: int, cost: int, lower: int, upper: int, tau: float, out: int) -> None:
+        _check(self.lib.prima_primal_step(self.h, x, kty, cost, lower, upper, tau, out))
+
+    def dual_step(self, y: int, kxbar: int, rhs: int, sigma: float, num_equalities: int, out: int) -> None:
+        _check(self.lib.prima_dual_step(self.h, y, kxbar, rhs, sigma, num_equalities, out))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class _Caps:
+    def __init__(self, name: str, device: str, supports_float64: bool):
+        self.name, self.device, self.supports_float64 = name, device, supports_float64
+
+    @property
+    def requires_double_precision_refinement(self) -> bool:
+        return not self.supports_float64
+
+
+def _solution(info: CInfo, x, y, rc) -> LpSolution:
+    sol = LpSolution(SolveStatus(info.status), x, y, rc, info.objective, info.dual_objective, info.iterations,
+                     info.restarts, int(info.solve_ms),
+                     KktError(info.primal_residual, info.dual_residual, info.objective, info.dual_objective),
+                     info.final_step_size, info.final_primal_weight)
+    sol.device_ms = info.device_ms
+    sol.setup_ms = info.setup_ms
+    sol.trials = info.trials
+    return sol
+
+
+def _warm(problem: LpProblem, ws: Optional[WarmStart]):
+    if ws is None:
+        return None, None
+    n, m = problem.num_variables, problem.num_constraints
+    if len(ws.primal) != n:
+        raise ValueError(f"requirement failed: warm start has {len(ws.primal)} primal entries, expected {n}")
+    if len(ws.dual) != m:
+        raise ValueError(f"requirement failed: warm start has {len(ws.dual)} dual entries, expected {m}")
+    px = np.ascontiguousarray(ws.primal, dtype=np.float64)
+    py = np.ascontiguousarray(ws.dual, dtype=np.float64)
+    w = CWarm(_dp(px), _dp(py), math.nan if ws.step_size is None else ws.step_size,
+              math.nan if ws.primal_weight is None else ws.primal_weight)
+    return w, (px, py)
+
+
+_ctx_cache: dict = {}
+_ctx_lock = threading.Lock()
+
+
+def context(device: int = 0, precision: int = 64) -> Context:
+    """A per-thread cached context (contexts are not thread-safe)."""
+    key = (threading.get_ident(), device, precision)
+    with _ctx_lock:
+        ctx = _ctx_cache.get(key)
+        if ctx is None or ctx._closed:
+            ctx = Context(device, precision)
+            _ctx_cache[key] = ctx
+    return ctx
+
+
+def solve(problem: LpProblem, params: PdhgParams = PdhgParams(), precision: int = 64,
+          warm_start: Optional[WarmStart] = None, cancel: Optional[C.c_int32] = None, device: int = 0,
+          ctx: Optional[Context] = None) -> LpSolution:
+    """``Pdhg.solveWith`` with the iteration resident on the GPU."""
+    ctx = ctx or context(device, precision)
+    lpv = _LpView(problem)
+    n, m = problem.num_variables, problem.num_constraints
+    x, y, rc = np.zeros(n), np.zeros(m), np.zeros(n)
+    warm, keep = _warm(problem, warm_start)
+    info = CInfo()
+    cp = to_c_params(params)
+    _check(ctx.lib.prima_pdhg_solve(ctx.handle, C.byref(lpv.c), C.byref(cp), None if warm is None else C.byref(warm),
+                                    None if cancel is None else C.cast(C.byref(cancel), _IP), _dp(x), _dp(y),
+                                    _dp(rc), C.byref(info)))
+    return _solution(info, x, y, rc)
+
+
+def to_c_mixed(mixed: MixedPrecisionParams, scheme: int = MIXED_REFINEMENT, max_refinements: int = 8,
+               refinement_growth: float = 1e4) -> CMixedParams:
+    return CMixedParams(mixed.reduced_tolerance, mixed.reduced_max_iterations, int(mixed.always_refine),
+                        mixed.reduced_time_share, scheme, max_refinements, refinement_growth)
+
+
+def mixed_solve(problem: LpProblem, params: PdhgParams = PdhgParams(),
+                mixed: MixedPrecisionParams = MixedPrecisionParams(), scheme: int = MIXED_REFINEMENT,
+                cancel: Optional[C.c_int32] = None, device: int = 0, max_refinements: int = 8,
+                refinement_growth: float = 1e4, ctx: Optional[Context] = None) -> MixedPrecisionResult:
+    """``MixedPrecision.solve`` with both passes on the GPU."""
+    ctx = ctx or context(device, 32)
+    lpv = _LpView(problem)
+    n, m = problem.num_variables, problem.num_constraints
+    x, y, rc = np.zeros(n), np.zeros(m), np.zeros(n)
+    info, minfo = CInfo(), CMixedInfo()
+    cp = to_c_params(params)
+    mp = to_c_mixed(mixed, scheme, max_refinements, refinement_growth)
+    _check(ctx.lib.prima_mixed_solve(ctx.handle, C.byref(lpv.c), C.byref(cp), C.byref(mp),
+                                     None if cancel is None else C.cast(C.byref(cancel), _IP), _dp(x), _dp(y),
+                                     _dp(rc), C.byref(info), C.byref(minfo)))
+    res = MixedPrecisionResult(_solution(info, x, y, rc), minfo.reduced_iterations, minfo.reduced_restarts,
+                               int(minfo.reduced_ms), minfo.refinement_iterations, int(minfo.refinement_ms),
+                               bool(minfo.refined), minfo.refinement_rounds)
+    return res
+
+
+def solve_batch(problems: Sequence[LpProblem], params: PdhgParams = PdhgParams(), precision: int = 64,
+                cancel: Optional[C.c_int32] = None, device: int = 0,
+                ctx: Optional[Context] = None) -> list[LpSolution]:
+    """``PrimaZio.solveAll``'s shape: every problem in one device launch."""
+    ctx = ctx or context(device, precision)
+    views = [_LpView(p) for p in problems]
+    arr = (CLp * len(problems))(*[v.c for v in views])
+    xs = [np.zeros(p.num_variables) for p in problems]
+    ys = [np.zeros(p.num_constraints) for p in problems]
+    rcs = [np.zeros(p.num_variables) for p in problems]
+    px = (_DP * len(problems))(*[_dp(a) for a in xs])
+    py = (_DP * len(problems))(*[_dp(a) for a in ys])
+    prc = (_DP * len(problems))(*[_dp(a) for a in rcs])
+    infos = (CInfo * len(problems))()
+    cp = to_c_params(params)
+    _check(ctx.lib.prima_pdhg_solve_batch(ctx.handle, len(problems), arr, C.byref(cp),
+                                          None if cancel is None else C.cast(C.byref(cancel), _IP), px, py, prc,
+                                          infos))
+    return [_solution(infos[i], xs[i], ys[i], rcs[i]) for i in range(len(problems))]

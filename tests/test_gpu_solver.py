@@ -1,0 +1,146 @@
+"""The device-resident solve (prima_pdhg_solve through the C ABI) against the
+oracle on the same seeded inputs: PdhgSuite (core/src/test/.../PdhgSuite.scala)
+and the validation ladder, in FP64 (ScalaKernels semantics) and FP32
+(Float32Kernels semantics).
+
+Tolerances: status identical; objective within 1e-8 relative of the oracle's
+FP64 answer at eps = 1e-9 (the ladder's worst-gap bound); on the ladder
+instances whose published trajectory is libm-insensitive the iteration and
+restart counts must match the oracle's exactly."""
+import ctypes
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from noaidi_b200.prima import LpProblem, PdhgParams, ScalingParams, SolveStatus, WarmStart
+from noaidi_b200.prima import generators as G
+from oracle import oracle as O
+from tests import lp_fixtures as F
+
+pytestmark = pytest.mark.gpu
+
+PINS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_pins.json")))
+P9 = PdhgParams(eps_abs=1e-9, eps_rel=1e-9, max_iterations=500_000)
+LADDER = F.ladder()
+
+
+def gpu_solve(problem, params=P9, precision=64, **kw):
+    from noaidi_b200.prima import cuda
+    return cuda.solve(problem, params, precision=precision, **kw)
+
+
+@pytest.mark.parametrize("entry", LADDER, ids=lambda e: e.name)
+def test_ladder_fp64_matches_oracle(entry):
+    ref = O.solve(entry.problem, P9)
+    got = gpu_solve(entry.problem)
+    assert got.status == ref.status == entry.expected
+    if ref.status == SolveStatus.OPTIMAL:
+        assert F.relative_gap(got.objective_value, ref.objective_value) <= 1e-8
+        assert np.allclose(got.primal, ref.primal, atol=1e-5 * max(1.0, np.abs(ref.primal).max()))
+    if entry.name in PINS["ladder_trajectory_exact"]:
+        assert (got.iterations, got.restarts) == (ref.iterations, ref.restarts)
+    else:
+        assert abs(got.iterations - ref.iterations) <= 0.25 * ref.iterations
+
+
+@pytest.mark.parametrize("entry", LADDER[:10], ids=lambda e: e.name)
+def test_ladder_fp32_matches_float32_oracle(entry):
+    p = PdhgParams(eps_abs=1e-5, eps_rel=1e-5, max_iterations=200_000, infeasibility_tolerance=1e-5)
+    ref = O.solve(entry.problem, p, mode=O.FP32)
+    got = gpu_solve(entry.problem, p, precision=32)
+    assert got.status == ref.status
+    if ref.status == SolveStatus.OPTIMAL:
+        assert F.relative_gap(got.objective_value, ref.objective_value) <= 1e-4
+
+
+def test_known_optima_and_congestion_prices():
+    for inst in F.optimal():
+        s = gpu_solve(inst.problem)
+        assert s.status == SolveStatus.OPTIMAL
+        assert s.objective_value == pytest.approx(inst.expected_objective, abs=1e-6 * max(1.0, abs(inst.expected_objective)))
+        for v, e in zip(s.primal, inst.expected_primal):
+            assert v == pytest.approx(e, abs=1e-5)
+        assert s.objective_value == pytest.approx(s.dual_objective_value, abs=1e-5 * max(1.0, abs(s.objective_value)))
+    s = gpu_solve(F.economic_dispatch().problem)
+    pin = PINS["fixtures"]["economic_dispatch_prices"]
+    assert s.dual[0] == pytest.approx(s.dual[1], abs=1e-4)
+    assert s.dual[2] == pytest.approx(pin["A2"], abs=pin["tolerance"])
+    assert s.dual[3] == pytest.approx(pin["B2"], abs=pin["tolerance"])
+
+
+def test_limits_trivial_and_statuses():
+    capped = gpu_solve(F.economic_dispatch().problem, PdhgParams(eps_abs=1e-14, eps_rel=1e-14, max_iterations=3))
+    assert capped.status == SolveStatus.ITERATION_LIMIT and capped.iterations == 3
+    ref = O.solve(F.economic_dispatch().problem, PdhgParams(eps_abs=1e-14, eps_rel=1e-14, max_iterations=3))
+    assert capped.objective_value == pytest.approx(ref.objective_value, rel=1e-12)
+    b = LpProblem.builder(2)
+    b.bounds(0, 0.0, 1.0).bounds(1, 0.0, 1.0)
+    triv = gpu_solve(b.build()[0])
+    assert triv.status == SolveStatus.OPTIMAL and triv.iterations == 0
+    timed = PdhgParams(eps_abs=1e-16, eps_rel=1e-16, max_iterations=50_000_000, time_limit_millis=50)
+    s = gpu_solve(F.random_feasible(5, 200, 40, 80), timed)
+    assert s.status == SolveStatus.TIME_LIMIT and s.iterations < 50_000_000
+
+
+def test_cancel_flag_is_polled_at_evaluation_points():
+    flag = ctypes.c_int32(1)
+    s = gpu_solve(F.random_feasible(5, 200, 40, 80), PdhgParams(eps_abs=1e-16, eps_rel=1e-16), cancel=flag)
+    assert s.status == SolveStatus.INTERRUPTED and s.iterations == 64
+
+
+def test_scaling_off_and_stability_bound():
+    unscaled = PdhgParams(eps_abs=1e-9, eps_rel=1e-9, scaling=ScalingParams.none())
+    for inst in F.optimal():
+        a, b = O.solve(inst.problem, unscaled), gpu_solve(inst.problem, unscaled)
+        assert a.status == b.status == SolveStatus.OPTIMAL
+        assert F.relative_gap(b.objective_value, a.objective_value) <= 1e-8
+    b = LpProblem.builder(1)
+    b.objective_coefficient(0, 1.0).bounds(0, 0.0, 10.0)
+    for _ in range(100):
+        b.greater_than([(0, 1.0)], 3.0)
+    s = gpu_solve(b.build()[0])
+    assert s.status == SolveStatus.OPTIMAL and s.objective_value == pytest.approx(3.0, abs=1e-6)
+
+
+def test_warm_starts():
+    p = F.economic_dispatch().problem
+    cold = gpu_solve(p)
+    warm = gpu_solve(p, warm_start=WarmStart.from_solution(cold))
+    assert warm.status == SolveStatus.OPTIMAL and warm.iterations < cold.iterations
+    ref = O.solve(p, P9, warm_start=WarmStart.from_solution(cold))
+    assert (warm.iterations, warm.restarts) == (ref.iterations, ref.restarts)
+    wild = WarmStart(np.array([1e6, -1e6]), np.array([-5.0]))
+    s = gpu_solve(F.equality_split().problem, warm_start=wild)
+    assert s.status == SolveStatus.OPTIMAL and s.objective_value == pytest.approx(24.0, abs=1e-6)
+    with pytest.raises(ValueError):
+        gpu_solve(F.equality_split().problem, warm_start=WarmStart(np.array([1.0]), np.array([0.0])))
+    with pytest.raises(ValueError):
+        gpu_solve(F.equality_split().problem, warm_start=WarmStart(np.array([math.nan, 1.0]), np.array([0.0])))
+
+
+def test_invalid_arguments_are_rejected():
+    with pytest.raises(ValueError):
+        gpu_solve(F.economic_dispatch().problem, PdhgParams.__new__(PdhgParams))
+
+
+@pytest.mark.parametrize("precision,eps", [(64, 1e-8), (32, 1e-5)], ids=["fp64", "fp32"])
+def test_lopf_matches_oracle(precision, eps):
+    P = G.dc_lopf(seed=3, buses=120, lines=180, generators=60, snapshots=6)
+    p = PdhgParams(eps_abs=eps, eps_rel=eps, max_iterations=400_000)
+    ref = O.solve(P, p, mode=O.FP64 if precision == 64 else O.FP32)
+    got = gpu_solve(P, p, precision=precision)
+    assert got.status == ref.status == SolveStatus.OPTIMAL
+    assert F.relative_gap(got.objective_value, ref.objective_value) <= (1e-8 if precision == 64 else 1e-4)
+    assert got.kkt.primal_residual_norm <= eps + eps * np.linalg.norm(P.rhs)
+    assert got.kkt.dual_residual_norm <= eps + eps * np.linalg.norm(P.objective)
+
+
+def test_config1_random_sparse_lp():
+    P = G.random_sparse_lp(0)
+    p = PdhgParams(eps_abs=1e-6, eps_rel=1e-6, max_iterations=400_000)
+    ref, got = O.solve(P, p), gpu_solve(P, p)
+    assert got.status == ref.status == SolveStatus.OPTIMAL
+    assert F.relative_gap(got.objective_value, ref.objective_value) <= 1e-5
