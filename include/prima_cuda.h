@@ -219,6 +219,26 @@ int32_t prima_pdhg_solve_batch(prima_handle ctx, int32_t count, const prima_lp *
                                double *const *primal_out, double *const *dual_out,
                                double *const *reduced_costs_out, prima_solution_info *infos);
 
+/* ---- device-resident problems ---------------------------------------------
+ * A problem uploaded and equilibrated once, then solved any number of times
+ * (warm-started passes, mixed-precision passes, repeated sweeps) without
+ * re-uploading or re-scaling.  The equilibration follows the ScalingParams in
+ * `params`; a solve whose params ask for a different scaling re-derives it.
+ * No counterpart in the reference, where LpProblem is a host object; this is
+ * the device residency the seam was designed for (Kernels.scala:33-37). */
+int32_t prima_problem_create(prima_handle ctx, const prima_lp *lp, const prima_params *params,
+                             prima_handle *problem);
+int32_t prima_problem_free(prima_handle ctx, prima_handle problem);
+/* As prima_pdhg_solve / prima_mixed_solve on a resident problem. */
+int32_t prima_problem_solve(prima_handle ctx, prima_handle problem, const prima_params *params,
+                            const prima_warm_start *warm_start, const volatile int32_t *cancel,
+                            double *primal_out, double *dual_out, double *reduced_costs_out,
+                            prima_solution_info *info);
+int32_t prima_problem_mixed_solve(prima_handle ctx, prima_handle problem, const prima_params *params,
+                                  const prima_mixed_params *mixed, const volatile int32_t *cancel,
+                                  double *primal_out, double *dual_out, double *reduced_costs_out,
+                                  prima_solution_info *info, prima_mixed_info *mixed_info);
+
 #ifdef __cplusplus
 }
 #endif

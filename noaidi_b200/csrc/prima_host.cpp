@@ -250,4 +250,80 @@ void prepare_scaled(const prima_lp *lp, const prima_params *p, ScaledLp *s) {
   s->scaled_q_norm = norm2(s->q.data(), m);
 }
 
+// Certificates.primalInfeasibility (Certificates.scala:60-123) and
+// dualInfeasibility (:137-195), classify (:207-219).
+int classify_fp64(const prima_lp *lp, const double *x, const double *y, double tol) {
+  const int32_t n = lp->num_variables, m = lp->num_constraints, neq = lp->num_equalities;
+  Csr K;
+  K.rows = m;
+  K.cols = n;
+  K.row_ptr.assign(lp->row_ptr, lp->row_ptr + m + 1);
+  K.col_idx.assign(lp->col_idx, lp->col_idx + K.row_ptr[m]);
+  K.vals.assign(lp->values, lp->values + K.row_ptr[m]);
+  Csr Kt;
+  csr_transpose(K, &Kt);
+  const double mn = spectral_norm_bound(K, Kt);
+  std::vector<double> kx((size_t)m), kty((size_t)n);
+  for (int32_t r = 0; r < m; r++) {
+    double acc = 0.0;
+    for (int32_t p = K.row_ptr[r]; p < K.row_ptr[r + 1]; p++) acc += K.vals[p] * x[K.col_idx[p]];
+    kx[r] = acc;
+  }
+  for (int32_t j = 0; j < n; j++) {
+    double acc = 0.0;
+    for (int32_t p = Kt.row_ptr[j]; p < Kt.row_ptr[j + 1]; p++) acc += Kt.vals[p] * y[Kt.col_idx[p]];
+    kty[j] = acc;
+  }
+  const double *q = lp->rhs, *c = lp->objective, *l = lp->lower, *u = lp->upper;
+  {  // primal infeasibility from y
+    double nsq = 0.0;
+    for (int32_t r = 0; r < m; r++) nsq += y[r] * y[r];
+    if (nsq > 0.0 && std::isfinite(nsq)) {
+      const double norm = std::sqrt(nsq);
+      double value = 0.0, rsq = 0.0, csq = 0.0;
+      for (int32_t r = 0; r < m; r++) value += q[r] * y[r];
+      for (int32_t j = 0; j < n; j++) {
+        const double rc = -kty[j];
+        if (rc > 0.0) {
+          if (std::isinf(l[j]) && l[j] < 0) rsq += rc * rc;
+          else value += l[j] * rc;
+        } else if (rc < 0.0) {
+          if (std::isinf(u[j]) && u[j] > 0) rsq += rc * rc;
+          else value += u[j] * rc;
+        }
+      }
+      for (int32_t r = neq; r < m; r++)
+        if (y[r] < 0.0) csq += y[r] * y[r];
+      if (value > 0.0 && std::isfinite(value)) {
+        const double rt = mn > 0.0 ? std::sqrt(rsq) / (mn * norm) : 0.0;
+        const double h = std::hypot(rt, std::sqrt(csq) / norm);
+        if (std::isfinite(h) && h <= tol) return PRIMA_STATUS_PRIMAL_INFEASIBLE;
+      }
+    }
+  }
+  {  // dual infeasibility from x
+    double nsq = 0.0;
+    for (int32_t j = 0; j < n; j++) nsq += x[j] * x[j];
+    if (nsq > 0.0 && std::isfinite(nsq)) {
+      const double norm = std::sqrt(nsq);
+      double value = 0.0;
+      for (int32_t j = 0; j < n; j++) value += c[j] * x[j];
+      if (value < 0.0 && std::isfinite(value)) {
+        double rowsq = 0.0, bsq = 0.0;
+        for (int32_t r = 0; r < m; r++)
+          if (r < neq || kx[r] < 0.0) rowsq += kx[r] * kx[r];
+        for (int32_t j = 0; j < n; j++) {
+          const double d = x[j];
+          if (d > 0.0 && !(std::isinf(u[j]) && u[j] > 0)) bsq += d * d;
+          else if (d < 0.0 && !(std::isinf(l[j]) && l[j] < 0)) bsq += d * d;
+        }
+        const double rt = mn > 0.0 ? std::sqrt(rowsq) / (mn * norm) : 0.0;
+        const double h = std::hypot(rt, std::sqrt(bsq) / norm);
+        if (std::isfinite(h) && h <= tol) return PRIMA_STATUS_DUAL_INFEASIBLE;
+      }
+    }
+  }
+  return -1;
+}
+
 }  // namespace prima

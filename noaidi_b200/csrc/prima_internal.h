@@ -58,6 +58,67 @@ struct Mat {
   int32_t lanes = 1;  // SpMV variant picked by the autotuner (1 = thread per row)
 };
 
+struct LpHostCopy;
+
+// A problem resident on the device: the original CSR and data, the
+// materialised transpose (as a permutation), the equilibrated matrix and
+// vectors in FP64, and per-precision copies for the solver.  Built once per
+// problem (prima_scaling.cu) and reused by every pass over it.
+struct PreparedLp {
+  int32_t n = 0, m = 0, neq = 0;
+  int64_t nnz = 0;
+  int32_t ruiz = -1, pc = -1;
+  double alpha = -1.0;
+  DeviceBuffer b_kp, b_kci, b_kv0, b_kv, b_tp, b_tci, b_perm;
+  DeviceBuffer b_c0, b_l0, b_u0, b_q0, b_cs, b_rs, b_sc, b_sl, b_su, b_sq;
+  struct PrecisionCopy {
+    DeviceBuffer kv, tv, c, l, u, q;
+  } copies[2];  // [0]: float, [1]: double
+  bool precision_ready[2] = {false, false};
+  double orig_spectral_bound = 0, scaled_spectral_bound = 0, rhs_norm = 0, obj_norm = 0;
+  double scaled_c_norm = 0, scaled_q_norm = 0;
+  std::vector<double> h_sc, h_sq, h_sl, h_su, h_cs, h_rs;  // host copies for warm starts
+  std::unique_ptr<LpHostCopy> owned;  // the caller's problem, when held by a handle
+  const prima_lp *host = nullptr;     // the caller's problem (valid while in use)
+
+  const int32_t *kp() const { return (const int32_t *)b_kp.ptr; }
+  const int32_t *kci() const { return (const int32_t *)b_kci.ptr; }
+  const double *kv0() const { return (const double *)b_kv0.ptr; }
+  double *kv() const { return (double *)b_kv.ptr; }
+  const int32_t *tp() const { return (const int32_t *)b_tp.ptr; }
+  const int32_t *tci() const { return (const int32_t *)b_tci.ptr; }
+  const int32_t *perm() const { return (const int32_t *)b_perm.ptr; }
+  const double *c0() const { return (const double *)b_c0.ptr; }
+  const double *l0() const { return (const double *)b_l0.ptr; }
+  const double *u0() const { return (const double *)b_u0.ptr; }
+  const double *q0() const { return (const double *)b_q0.ptr; }
+  const double *cs() const { return (const double *)b_cs.ptr; }
+  const double *rs() const { return (const double *)b_rs.ptr; }
+  double *cs_() const { return (double *)b_cs.ptr; }
+  double *rs_() const { return (double *)b_rs.ptr; }
+  const double *sc() const { return (const double *)b_sc.ptr; }
+  const double *sl() const { return (const double *)b_sl.ptr; }
+  const double *su() const { return (const double *)b_su.ptr; }
+  const double *sq() const { return (const double *)b_sq.ptr; }
+  double *sc_() const { return (double *)b_sc.ptr; }
+  double *sl_() const { return (double *)b_sl.ptr; }
+  double *su_() const { return (double *)b_su.ptr; }
+  double *sq_() const { return (double *)b_sq.ptr; }
+  bool scaled_like(const prima_params *p) const {
+    return ruiz == p->ruiz_iterations && pc == p->apply_pock_chambolle && alpha == p->pock_chambolle_alpha;
+  }
+  int32_t prepare(const prima_lp *lp, const prima_params *p, cudaStream_t s);
+  template <typename T>
+  int32_t materialise(cudaStream_t s);
+};
+
+// Owned host copy of a problem (for problem handles).
+struct LpHostCopy {
+  std::vector<int32_t> row_ptr, col_idx;
+  std::vector<double> values, objective, rhs, lower, upper;
+  prima_lp lp;
+};
+
 struct Ctx {
   int32_t device = 0;
   int32_t bits = 64;
@@ -73,6 +134,8 @@ struct Ctx {
   int32_t *cancel_mapped = nullptr;  // pinned + mapped: cancel flag seen by the device
   int32_t *cancel_mapped_dev = nullptr;
   DeviceBuffer solver_arena;   // buffers of the coarse solvers, reused across solves
+  PreparedLp scratch_lp;       // the problem of a one-shot solve call
+  std::unordered_map<int64_t, std::unique_ptr<PreparedLp>> problems;
 };
 
 // Registry lookup (thread-safe); returns nullptr and sets the error on failure.
@@ -108,6 +171,11 @@ void prepare_scaled(const prima_lp *lp, const prima_params *p, ScaledLp *out);
 void csr_transpose(const Csr &a, Csr *t);
 double csr_norm_inf(const Csr &a);
 double spectral_norm_bound(const Csr &a, const Csr &at);
+
+// Certificates.classify (Certificates.scala:207-219) in FP64 on the host,
+// recomputing Kx and K'y from the original matrix (the re-check
+// MixedPrecision.scala:143-152 performs).  Returns a PRIMA_STATUS_* or -1.
+int classify_fp64(const prima_lp *lp, const double *x, const double *y, double tolerance);
 
 // ---- SpMV helpers for the seam (prima_ops.cu) ------------------------------
 int32_t seam_spmv(Ctx *ctx, const Mat *a, const void *x, void *out);

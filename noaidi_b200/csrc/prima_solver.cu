@@ -38,7 +38,8 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
 }
 
 // Data written inside this launch by other blocks is read through L2 only
-// (ld.global.cg), so no stale L1 line can be observed across a barrier.
+// (ld.global.cg), so no stale L1 line can be observed across a barrier;
+// data that never changes during the launch goes through the read-only path.
 template <typename T>
 __device__ __forceinline__ T ldv(const T *p) {
   return __ldcg(p);
@@ -54,60 +55,117 @@ __device__ __forceinline__ void chunk(int32_t total, int nb, int rank, int32_t &
   hi = (int32_t)b;
 }
 
-// Row r of a CSR matrix against a vector written in this launch, summed in
-// index order from zero (SparseMatrix.multiplyInto order).
-template <typename T>
-__device__ __forceinline__ T row_dot(const int32_t *__restrict__ p, const int32_t *__restrict__ ci,
-                                     const T *__restrict__ v, const T *x, int32_t r) {
-  T acc = T(0);
-  const int32_t e = __ldg(p + r + 1);
-  for (int32_t k = __ldg(p + r); k < e; k++) acc = acc + (__ldg(v + k) * ldv(x + __ldg(ci + k)));
-  return acc;
+// CSR-stream SpMV over the block's rows [lo, hi), one tile of kTileRows rows
+// at a time.  Stage 1: the tile's products v[k] * x[col[k]] (rounded to T)
+// are formed with coalesced matrix loads and fully parallel gathers into
+// shared memory.  Stage 2: each thread sums its rows' products in index
+// order starting from zero -- the reference's per-row order, bit for bit --
+// and hands (row, acc, prefetched operands) to the epilogue.  The epilogue's
+// own operands are loaded by `pre` before stage 1, so their latency overlaps
+// the gathers.  A tile with more than kTileCap entries is summed straight
+// from global memory in the same order.
+template <typename T, typename Pre, typename Epi>
+__device__ __forceinline__ void csr_tiles(int32_t lo, int32_t hi, const int32_t *__restrict__ p,
+                                          const int32_t *__restrict__ ci, const T *__restrict__ v, const T *x,
+                                          T *s_prod, Pre &&pre, Epi &&epi) {
+  using Ops = decltype(pre(0));
+  int32_t k0 = lo < hi ? __ldg(p + lo) : 0;
+  for (int32_t r0 = lo; r0 < hi; r0 += kTileRows) {
+    const int32_t r1 = min(hi, r0 + kTileRows);
+    Ops ops[kRowsPerThread];
+    int32_t ra[kRowsPerThread], rb[kRowsPerThread];
+#pragma unroll
+    for (int i = 0; i < kRowsPerThread; i++) {
+      const int32_t r = r0 + threadIdx.x + i * kThreads;
+      if (r < r1) {
+        ops[i] = pre(r);
+        ra[i] = __ldg(p + r);
+        rb[i] = __ldg(p + r + 1);
+      }
+    }
+    const int32_t k1 = __ldg(p + r1);
+    const bool staged = (k1 - k0) <= kTileCap;
+    if (staged) {
+#pragma unroll 4
+      for (int32_t k = k0 + threadIdx.x; k < k1; k += kThreads) s_prod[k - k0] = __ldg(v + k) * ldv(x + __ldg(ci + k));
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kRowsPerThread; i++) {
+      const int32_t r = r0 + threadIdx.x + i * kThreads;
+      if (r < r1) {
+        T acc = T(0);
+        if (staged) {
+          for (int32_t k = ra[i]; k < rb[i]; k++) acc = acc + s_prod[k - k0];
+        } else {
+          for (int32_t k = ra[i]; k < rb[i]; k++) acc = acc + (__ldg(v + k) * ldv(x + __ldg(ci + k)));
+        }
+        epi(r, acc, ops[i]);
+      }
+    }
+    k0 = k1;
+    __syncthreads();
+  }
 }
 
-// Block-wide sum of Q per-thread values in a fixed order; thread 0 stores the
-// block's partials at partials[q * stride + rank].
+struct None {};
+
+// Block-wide totals of Q per-thread values in a fixed order.  The block's
+// totals go to shared s_part[base..base+Q) and, in a multi-block team, to the
+// global partials[(base + q) * stride + rank].
 template <int Q>
-__device__ __forceinline__ void block_partials(double (&v)[Q], double *partials, int stride, int rank) {
+__device__ __forceinline__ void block_partials(const double (&v)[Q], double *partials, int stride, int rank, int nb,
+                                               int base, double *s_part) {
   __shared__ double sh[kMaxQ][kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < Q; q++) {
     double s = v[q];
+#pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) sh[q][warp] = s;
   }
   __syncthreads();
   if (threadIdx.x < Q) {
     double s = 0.0;
+#pragma unroll
     for (int w = 0; w < kWarps; w++) s += sh[threadIdx.x][w];
-    partials[threadIdx.x * stride + rank] = s;
+    s_part[base + threadIdx.x] = s;
+    if (nb > 1) partials[(base + threadIdx.x) * stride + rank] = s;
   }
   __syncthreads();
 }
 
-// Deciding block: total of slots [q0, q0+Q) over nb block partials, fixed order.
+// Deciding block: totals of slots [0, Q) over the nb block partials, in a
+// fixed order (the block's own shared totals when nb == 1).
 template <int Q>
-__device__ __forceinline__ void reduce_partials(const double *partials, int stride, int nb, int q0,
-                                                double *out /* shared, Q */) {
+__device__ __forceinline__ void reduce_partials(const double *partials, int stride, int nb, const double *s_part,
+                                                double *out) {
+  if (nb == 1) {
+    if (threadIdx.x < Q) out[threadIdx.x] = s_part[threadIdx.x];
+    __syncthreads();
+    return;
+  }
   __shared__ double sh[kMaxQ][kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double v[Q];
 #pragma unroll
   for (int q = 0; q < Q; q++) {
     double s = 0.0;
-    for (int b = threadIdx.x; b < nb; b += kThreads) s += ldv(partials + (q0 + q) * stride + b);
+    for (int b = threadIdx.x; b < nb; b += kThreads) s += ldv(partials + q * stride + b);
     v[q] = s;
   }
 #pragma unroll
   for (int q = 0; q < Q; q++) {
     double s = v[q];
+#pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) sh[q][warp] = s;
   }
   __syncthreads();
   if (threadIdx.x < Q) {
     double s = 0.0;
+#pragma unroll
     for (int w = 0; w < kWarps; w++) s += sh[threadIdx.x][w];
     out[threadIdx.x] = s;
   }
@@ -215,80 +273,10 @@ __device__ void after_checkpoint(Control &c, const Kkt &point, const Params &P, 
   }
 }
 
-// ---- the team barrier -------------------------------------------------------
-
-constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~seconds; a phase takes microseconds
-
-template <typename T>
-__device__ void decide(const Args<T> &a, Control &c, int phase, int nb, double *red);
-
-// All blocks arrive; the last one reduces and decides, then releases.  Every
-// wait is bounded: on timeout the team's abort flag is raised, the kernel
-// records PRIMA_ERR_TIMEOUT and every block leaves.
-template <typename T>
-__device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, int nb) {
-  __shared__ unsigned s_gen;
-  __shared__ int s_last, s_ok;
-  __shared__ double s_red[kMaxQ];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    s_gen = ld_acquire(&a.sync->gen);
-    __threadfence();
-    const unsigned old = atom_add_acq_rel(&a.sync->count, 1u);
-    s_last = old == (unsigned)(nb - 1);
-    s_ok = 1;
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    decide<T>(a, snap, phase, nb, s_red);  // block-wide; thread 0 updates snap
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      if (*((volatile int32_t *)&a.sync->abort)) {
-        snap.error = PRIMA_ERR_TIMEOUT;
-        snap.phase = PH_DONE;
-      }
-      // publish the new control record, then release the team
-      const unsigned *src = (const unsigned *)&snap;
-      unsigned *dst = (unsigned *)a.ctl;
-      for (int i = 0; i < (int)(sizeof(Control) / 4); i++) dst[i] = src[i];
-      a.sync->count = 0;
-      __threadfence();
-      st_release(&a.sync->gen, s_gen + 1);
-    }
-  } else if (threadIdx.x == 0) {
-    unsigned long long spins = 0;
-    while (ld_acquire(&a.sync->gen) == s_gen) {
-      if (*((volatile int32_t *)&a.sync->abort)) {
-        s_ok = 0;
-        break;
-      }
-      if (++spins > kSpinLimit) {
-        atomicExch(&a.sync->abort, 1);
-        a.ctl->error = PRIMA_ERR_TIMEOUT;
-        s_ok = 0;
-        break;
-      }
-      __nanosleep(32);
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return s_ok;
-}
-
-template <typename T>
-__device__ __forceinline__ void load_control(const Args<T> &a, Control &snap) {
-  const unsigned *src = (const unsigned *)a.ctl;
-  unsigned *dst = (unsigned *)&snap;
-  for (int i = threadIdx.x; i < (int)(sizeof(Control) / 4); i += blockDim.x) dst[i] = __ldcg(src + i);
-  __syncthreads();
-}
-
 // ---- evaluation terms --------------------------------------------------------
 
-// Row r: current point terms (Kkt.evaluate rows, certificate rows).
-__device__ __forceinline__ void eval_row(double yv, double kxv, double rs, double q0, bool eq, double *v) {
+// Row r: Kkt.evaluate's primal residual and q'y; the certificates' row terms.
+__device__ __forceinline__ void eval_row(double yv, double kxv, double rs, double q0, bool eq, double (&v)[kRowQ]) {
   const double yo = yv * rs, kxo = kxv / rs;
   if (eq) {
     const double d = kxo - q0;
@@ -304,7 +292,8 @@ __device__ __forceinline__ void eval_row(double yv, double kxv, double rs, doubl
   v[Q_YSQ] += yo * yo;
 }
 
-__device__ __forceinline__ void eval_row_avg(double yv, double kxv, double rs, double q0, bool eq, double *v) {
+__device__ __forceinline__ void eval_row_avg(double yv, double kxv, double rs, double q0, bool eq,
+                                             double (&v)[kRowQ]) {
   const double yo = yv * rs, kxo = kxv / rs;
   if (eq) {
     const double d = kxo - q0;
@@ -316,132 +305,161 @@ __device__ __forceinline__ void eval_row_avg(double yv, double kxv, double rs, d
   v[Q_A_QY] += q0 * yo;
 }
 
-// Column j: current point terms (Kkt.evaluate columns, certificate columns).
+// Column j: Kkt.evaluate's objective and dual terms; the certificates'
+// column terms.  Indices are slot - Q_CX.
 __device__ __forceinline__ void eval_col(double xv, double ktv, double cs, double c0, double l0, double u0,
-                                         double *v) {
+                                         double (&v)[kColQ]) {
   const double xo = xv * cs, kto = ktv / cs;
   const bool lfin = !(isinf(l0) && l0 < 0.0), ufin = !(isinf(u0) && u0 > 0.0);
-  v[Q_CX] += c0 * xo;
+  v[Q_CX - Q_CX] += c0 * xo;
   const double rc = c0 - kto;
   if (rc > 0.0) {
-    if (!lfin) v[Q_DSQ] += rc * rc;
-    else v[Q_DTERM] += l0 * rc;
+    if (!lfin) v[Q_DSQ - Q_CX] += rc * rc;
+    else v[Q_DTERM - Q_CX] += l0 * rc;
   } else if (rc < 0.0) {
-    if (!ufin) v[Q_DSQ] += rc * rc;
-    else v[Q_DTERM] += u0 * rc;
+    if (!ufin) v[Q_DSQ - Q_CX] += rc * rc;
+    else v[Q_DTERM - Q_CX] += u0 * rc;
   }
   const double pr = -kto;
   if (pr > 0.0) {
-    if (!lfin) v[Q_PRSQ] += pr * pr;
-    else v[Q_PVAL] += l0 * pr;
+    if (!lfin) v[Q_PRSQ - Q_CX] += pr * pr;
+    else v[Q_PVAL - Q_CX] += l0 * pr;
   } else if (pr < 0.0) {
-    if (!ufin) v[Q_PRSQ] += pr * pr;
-    else v[Q_PVAL] += u0 * pr;
+    if (!ufin) v[Q_PRSQ - Q_CX] += pr * pr;
+    else v[Q_PVAL - Q_CX] += u0 * pr;
   }
-  v[Q_XSQ] += xo * xo;
-  if ((xo > 0.0 && ufin) || (xo < 0.0 && lfin)) v[Q_BSQ] += xo * xo;
+  v[Q_XSQ - Q_CX] += xo * xo;
+  if ((xo > 0.0 && ufin) || (xo < 0.0 && lfin)) v[Q_BSQ - Q_CX] += xo * xo;
 }
 
 __device__ __forceinline__ void eval_col_avg(double xv, double ktv, double cs, double c0, double l0, double u0,
-                                             double *v) {
+                                             double (&v)[kColQ]) {
   const double xo = xv * cs, kto = ktv / cs;
-  v[Q_A_CX] += c0 * xo;
+  v[Q_A_CX - Q_CX] += c0 * xo;
   const double rc = c0 - kto;
   if (rc > 0.0) {
-    if (isinf(l0) && l0 < 0.0) v[Q_A_DSQ] += rc * rc;
-    else v[Q_A_DTERM] += l0 * rc;
+    if (isinf(l0) && l0 < 0.0) v[Q_A_DSQ - Q_CX] += rc * rc;
+    else v[Q_A_DTERM - Q_CX] += l0 * rc;
   } else if (rc < 0.0) {
-    if (isinf(u0) && u0 > 0.0) v[Q_A_DSQ] += rc * rc;
-    else v[Q_A_DTERM] += u0 * rc;
+    if (isinf(u0) && u0 > 0.0) v[Q_A_DSQ - Q_CX] += rc * rc;
+    else v[Q_A_DTERM - Q_CX] += u0 * rc;
   }
 }
 
 // ---- phases --------------------------------------------------------------------
 
+struct Team {
+  int nb, rank;
+  double *s_part;  // shared: this block's totals, by slot
+};
+
 template <typename T>
-__device__ void phase_init(const Args<T> &a, const Control &s, int nb, int rank) {
-  double v[kMaxQ];
-#pragma unroll
-  for (int q = 0; q < kMaxQ; q++) v[q] = 0.0;
+__device__ void phase_init(const Args<T> &a, const Control &s, const Team &tm, T *s_prod) {
   int32_t lo, hi;
-  chunk(a.n, nb, rank, lo, hi);
-  for (int32_t j = lo + threadIdx.x; j < hi; j += kThreads) {
-    const T xj = ldv(a.x[0] + j);
-    const T kt = row_dot(a.tp, a.tci, a.tv, (const T *)a.y[0], j);
-    a.kty[j] = kt;
-    a.xr[j] = xj;
-    a.sx[j] = T(0);
-    a.skty[j] = T(0);
-    eval_col((double)xj, (double)kt, __ldg(a.cs + j), __ldg(a.c0 + j), __ldg(a.l0 + j), __ldg(a.u0 + j), v);
+  {
+    double v[kColQ];
+#pragma unroll
+    for (int q = 0; q < kColQ; q++) v[q] = 0.0;
+    chunk(a.n, tm.nb, tm.rank, lo, hi);
+    csr_tiles<T>(lo, hi, a.tp, a.tci, a.tv, (const T *)a.y[0], s_prod, [&](int32_t) { return None{}; },
+                 [&](int32_t j, T kt, None) {
+      const T xj = ldv(a.x[0] + j);
+      a.kty[j] = kt;
+      a.xr[j] = xj;
+      a.sx[j] = T(0);
+      a.skty[j] = T(0);
+      eval_col((double)xj, (double)kt, __ldg(a.cs + j), __ldg(a.c0 + j), __ldg(a.l0 + j), __ldg(a.u0 + j), v);
+    });
+    block_partials<kColQ>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_CX, tm.s_part);
   }
-  chunk(a.m, nb, rank, lo, hi);
-  for (int32_t r = lo + threadIdx.x; r < hi; r += kThreads) {
-    const T yv = ldv(a.y[0] + r);
-    const T kxv = row_dot(a.kp, a.kci, a.kv, (const T *)a.x[0], r);
-    a.kx[0][r] = kxv;
-    a.yr[r] = yv;
-    a.sy[r] = T(0);
-    a.skx[r] = T(0);
-    eval_row((double)yv, (double)kxv, __ldg(a.rs + r), __ldg(a.q0 + r), r < a.neq, v);
+  {
+    double v[kRowQ];
+#pragma unroll
+    for (int q = 0; q < kRowQ; q++) v[q] = 0.0;
+    chunk(a.m, tm.nb, tm.rank, lo, hi);
+    csr_tiles<T>(lo, hi, a.kp, a.kci, a.kv, (const T *)a.x[0], s_prod, [&](int32_t) { return None{}; },
+                 [&](int32_t r, T kxv, None) {
+      const T yv = ldv(a.y[0] + r);
+      a.kx[0][r] = kxv;
+      a.yr[r] = yv;
+      a.sy[r] = T(0);
+      a.skx[r] = T(0);
+      eval_row((double)yv, (double)kxv, __ldg(a.rs + r), __ldg(a.q0 + r), r < a.neq, v);
+    });
+    block_partials<kRowQ>(v, a.partials, a.max_blocks, tm.rank, tm.nb, 0, tm.s_part);
   }
-  block_partials<kMaxQ>(v, a.partials, a.max_blocks, rank);
 }
 
-// Primal half of a trial, fused with the pending commit's K'y.
+// Primal half of a trial (primalStep + extrapolation), fused with the
+// pending commit's K'y and running sums.
 template <typename T>
-__device__ void phase_a(const Args<T> &a, const Control &s, int nb, int rank) {
+__device__ void phase_a(const Args<T> &a, const Control &s, const Team &tm, T *s_prod) {
   double v[1] = {0.0};
   int32_t lo, hi;
-  chunk(a.n, nb, rank, lo, hi);
+  chunk(a.n, tm.nb, tm.rank, lo, hi);
   const T tau = (T)s.tau, w = (T)s.pend_w;
   const T *x = a.x[s.xc];
   T *xn_out = a.x[s.xc ^ 1];
-  const T *y = a.y[s.yc];
-  const bool pend = s.pend != 0;
-  for (int32_t j = lo + threadIdx.x; j < hi; j += kThreads) {
-    const T xj = ldv(x + j);
-    T kt;
-    if (pend) {
-      kt = row_dot(a.tp, a.tci, a.tv, y, j);
-      a.kty[j] = kt;
-      a.sx[j] = (w * xj) + (T(1) * ldv(a.sx + j));
-      a.skty[j] = (w * kt) + (T(1) * ldv(a.skty + j));
-    } else {
-      kt = ldv(a.kty + j);
-    }
-    // primalStep (ScalaKernels.scala:78-98), two-comparison clamp
-    const T step = xj - (tau * (__ldg(a.c + j) - kt));
+  auto step = [&](int32_t j, T xj, T kt) {
+    // ScalaKernels.primalStep (:78-98): two-comparison clamp
+    const T st = xj - (tau * (__ldg(a.c + j) - kt));
     const T lj = __ldg(a.l + j), uj = __ldg(a.u + j);
-    const T xn = step < lj ? lj : (step > uj ? uj : step);
+    const T xn = st < lj ? lj : (st > uj ? uj : st);
     xn_out[j] = xn;
     a.xbar[j] = (T(2) * xn) + (T(-1) * xj);
     const T d = (T(1) * xn) + (T(-1) * xj);
     v[0] += (double)d * (double)d;
+  };
+  if (s.pend) {
+    struct Ops {
+      T x, sx, skty;
+    };
+    csr_tiles<T>(lo, hi, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], s_prod,
+                 [&](int32_t j) { return Ops{ldv(x + j), ldv(a.sx + j), ldv(a.skty + j)}; },
+                 [&](int32_t j, T kt, const Ops &o) {
+      a.kty[j] = kt;
+      a.sx[j] = (w * o.x) + (T(1) * o.sx);
+      a.skty[j] = (w * kt) + (T(1) * o.skty);
+      step(j, o.x, kt);
+    });
+  } else {
+    for (int32_t j = lo + threadIdx.x; j < hi; j += kThreads) step(j, ldv(x + j), ldv(a.kty + j));
   }
-  block_partials<1>(v, a.partials + Q_DX * a.max_blocks, a.max_blocks, rank);
+  block_partials<1>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DX, tm.s_part);
 }
 
-// Dual half of a trial: K xbar, dual step, speculative kx commit value.
+// Dual half of a trial: K xbar, dualStep, the speculative kx commit value.
 template <typename T>
-__device__ void phase_b(const Args<T> &a, const Control &s, int nb, int rank) {
+__device__ void phase_b(const Args<T> &a, const Control &s, const Team &tm, T *s_prod) {
   double v[2] = {0.0, 0.0};
   int32_t lo, hi;
-  chunk(a.m, nb, rank, lo, hi);
+  chunk(a.m, tm.nb, tm.rank, lo, hi);
   const T sigma = (T)s.sigma, w = (T)s.pend_w;
   const T *y = a.y[s.yc];
   const T *kx = a.kx[s.kxc];
   T *y_out = a.y[s.yc ^ 1];
   T *kx_out = a.kx[s.kxc ^ 1];
   const bool pend = s.pend != 0;
-  for (int32_t r = lo + threadIdx.x; r < hi; r += kThreads) {
-    const T yr = ldv(y + r), kxr = ldv(kx + r);
+  struct Ops {
+    T y, kx, q, sy, skx;
+  };
+  csr_tiles<T>(lo, hi, a.kp, a.kci, a.kv, (const T *)a.xbar, s_prod,
+               [&](int32_t r) {
+                 Ops o{ldv(y + r), ldv(kx + r), __ldg(a.q + r), T(0), T(0)};
+                 if (pend) {
+                   o.sy = ldv(a.sy + r);
+                   o.skx = ldv(a.skx + r);
+                 }
+                 return o;
+               },
+               [&](int32_t r, T kb, const Ops &o) {
+    const T yr = o.y, kxr = o.kx;
     if (pend) {
-      a.sy[r] = (w * yr) + (T(1) * ldv(a.sy + r));
-      a.skx[r] = (w * kxr) + (T(1) * ldv(a.skx + r));
+      a.sy[r] = (w * yr) + (T(1) * o.sy);
+      a.skx[r] = (w * kxr) + (T(1) * o.skx);
     }
-    const T kb = row_dot(a.kp, a.kci, a.kv, (const T *)a.xbar, r);
-    // dualStep (ScalaKernels.scala:100-118)
-    T yn = yr + (sigma * (__ldg(a.q + r) - kb));
+    // ScalaKernels.dualStep (:100-118)
+    T yn = yr + (sigma * (o.q - kb));
     if (r >= a.neq) yn = yn > T(0) ? yn : T(0);
     y_out[r] = yn;
     kx_out[r] = (T(0.5) * kb) + (T(0.5) * kxr);
@@ -449,67 +467,81 @@ __device__ void phase_b(const Args<T> &a, const Control &s, int nb, int rank) {
     const T kdx = (T(0.5) * kb) + (T(-0.5) * kxr);
     v[0] += (double)dy * (double)dy;
     v[1] += (double)dy * (double)kdx;
-  }
-  block_partials<2>(v, a.partials + Q_DY * a.max_blocks, a.max_blocks, rank);
+  });
+  block_partials<2>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DY, tm.s_part);
 }
 
-// Flush the pending commit, optionally refresh kx = K x, evaluate.
+// Flush the pending commit, optionally refresh kx = K x, evaluate the
+// current point and the running average.
 template <typename T>
-__device__ void phase_f(const Args<T> &a, const Control &s, int nb, int rank) {
-  double v[kMaxQ];
-#pragma unroll
-  for (int q = 0; q < kMaxQ; q++) v[q] = 0.0;
+__device__ void phase_f(const Args<T> &a, const Control &s, const Team &tm, T *s_prod) {
   const T w = (T)s.pend_w, inv = (T)s.inv_w;
   const bool pend = s.pend != 0, fresh = s.f_mode != F_ITERLIMIT, avg = s.f_avg != 0;
   const T *x = a.x[s.xc];
   const T *y = a.y[s.yc];
   T *kx = a.kx[s.kxc];
   int32_t lo, hi;
-  chunk(a.n, nb, rank, lo, hi);
-  for (int32_t j = lo + threadIdx.x; j < hi; j += kThreads) {
-    const T xj = ldv(x + j);
-    T kt;
+  {
+    double v[kColQ];
+#pragma unroll
+    for (int q = 0; q < kColQ; q++) v[q] = 0.0;
+    chunk(a.n, tm.nb, tm.rank, lo, hi);
+    auto col = [&](int32_t j, T kt) {
+      const T xj = ldv(x + j);
+      const double cs = __ldg(a.cs + j), c0 = __ldg(a.c0 + j), l0 = __ldg(a.l0 + j), u0 = __ldg(a.u0 + j);
+      eval_col((double)xj, (double)kt, cs, c0, l0, u0, v);
+      if (avg) eval_col_avg((double)(inv * ldv(a.sx + j)), (double)(inv * ldv(a.skty + j)), cs, c0, l0, u0, v);
+    };
     if (pend) {
-      kt = row_dot(a.tp, a.tci, a.tv, y, j);
-      a.kty[j] = kt;
-      a.sx[j] = (w * xj) + (T(1) * ldv(a.sx + j));
-      a.skty[j] = (w * kt) + (T(1) * ldv(a.skty + j));
+      csr_tiles<T>(lo, hi, a.tp, a.tci, a.tv, y, s_prod, [&](int32_t) { return None{}; }, [&](int32_t j, T kt, None) {
+        const T xj = ldv(x + j);
+        a.kty[j] = kt;
+        a.sx[j] = (w * xj) + (T(1) * ldv(a.sx + j));
+        a.skty[j] = (w * kt) + (T(1) * ldv(a.skty + j));
+        col(j, kt);
+      });
     } else {
-      kt = ldv(a.kty + j);
+      for (int32_t j = lo + threadIdx.x; j < hi; j += kThreads) col(j, ldv(a.kty + j));
     }
-    const double cs = __ldg(a.cs + j), c0 = __ldg(a.c0 + j), l0 = __ldg(a.l0 + j), u0 = __ldg(a.u0 + j);
-    eval_col((double)xj, (double)kt, cs, c0, l0, u0, v);
-    if (avg) {
-      const T ax = inv * ldv(a.sx + j), akt = inv * ldv(a.skty + j);
-      eval_col_avg((double)ax, (double)akt, cs, c0, l0, u0, v);
-    }
+    block_partials<kColQ>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_CX, tm.s_part);
   }
-  chunk(a.m, nb, rank, lo, hi);
-  for (int32_t r = lo + threadIdx.x; r < hi; r += kThreads) {
-    const T yr = ldv(y + r);
-    T kxr = ldv(kx + r);
-    if (pend) {
-      a.sy[r] = (w * yr) + (T(1) * ldv(a.sy + r));
-      a.skx[r] = (w * kxr) + (T(1) * ldv(a.skx + r));
-    }
+  {
+    double v[kRowQ];
+#pragma unroll
+    for (int q = 0; q < kRowQ; q++) v[q] = 0.0;
+    chunk(a.m, tm.nb, tm.rank, lo, hi);
+    auto row = [&](int32_t r, T kxr) {
+      const T yr = ldv(y + r);
+      const double rs = __ldg(a.rs + r), q0 = __ldg(a.q0 + r);
+      eval_row((double)yr, (double)kxr, rs, q0, r < a.neq, v);
+      if (avg) eval_row_avg((double)(inv * ldv(a.sy + r)), (double)(inv * ldv(a.skx + r)), rs, q0, r < a.neq, v);
+    };
+    auto flush = [&](int32_t r) {
+      if (pend) {
+        a.sy[r] = (w * ldv(y + r)) + (T(1) * ldv(a.sy + r));
+        a.skx[r] = (w * ldv(kx + r)) + (T(1) * ldv(a.skx + r));
+      }
+    };
     if (fresh) {
-      kxr = row_dot(a.kp, a.kci, a.kv, x, r);
-      kx[r] = kxr;
+      csr_tiles<T>(lo, hi, a.kp, a.kci, a.kv, x, s_prod, [&](int32_t) { return None{}; }, [&](int32_t r, T kxr, None) {
+        flush(r);  // the running sum takes the incremental kx, then the fresh one replaces it
+        kx[r] = kxr;
+        row(r, kxr);
+      });
+    } else {
+      for (int32_t r = lo + threadIdx.x; r < hi; r += kThreads) {
+        flush(r);
+        row(r, ldv(kx + r));
+      }
     }
-    const double rs = __ldg(a.rs + r), q0 = __ldg(a.q0 + r);
-    eval_row((double)yr, (double)kxr, rs, q0, r < a.neq, v);
-    if (avg) {
-      const T ay = inv * ldv(a.sy + r), akx = inv * ldv(a.skx + r);
-      eval_row_avg((double)ay, (double)akx, rs, q0, r < a.neq, v);
-    }
+    block_partials<kRowQ>(v, a.partials, a.max_blocks, tm.rank, tm.nb, 0, tm.s_part);
   }
-  block_partials<kMaxQ>(v, a.partials, a.max_blocks, rank);
 }
 
 // restartAt (Pdhg.scala:478-502): adopt the average if chosen, measure the
 // distance travelled since the last restart, re-centre, reset the sums.
 template <typename T>
-__device__ void phase_r(const Args<T> &a, const Control &s, int nb, int rank) {
+__device__ void phase_r(const Args<T> &a, const Control &s, const Team &tm) {
   double v[2] = {0.0, 0.0};
   const T inv = (T)s.inv_w;
   const bool avg = s.r_avg != 0;
@@ -517,7 +549,7 @@ __device__ void phase_r(const Args<T> &a, const Control &s, int nb, int rank) {
   T *y = a.y[s.yc];
   T *kx = a.kx[s.kxc];
   int32_t lo, hi;
-  chunk(a.n, nb, rank, lo, hi);
+  chunk(a.n, tm.nb, tm.rank, lo, hi);
   for (int32_t j = lo + threadIdx.x; j < hi; j += kThreads) {
     T xj;
     if (avg) {
@@ -533,7 +565,7 @@ __device__ void phase_r(const Args<T> &a, const Control &s, int nb, int rank) {
     a.sx[j] = T(0);
     a.skty[j] = T(0);
   }
-  chunk(a.m, nb, rank, lo, hi);
+  chunk(a.m, tm.nb, tm.rank, lo, hi);
   for (int32_t r = lo + threadIdx.x; r < hi; r += kThreads) {
     T yr;
     if (avg) {
@@ -549,19 +581,19 @@ __device__ void phase_r(const Args<T> &a, const Control &s, int nb, int rank) {
     a.sy[r] = T(0);
     a.skx[r] = T(0);
   }
-  block_partials<2>(v, a.partials, a.max_blocks, rank);
+  block_partials<2>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DXR, tm.s_part);
 }
 
 // finish (Pdhg.scala:510-532): the evaluated point in the caller's units and
 // the reduced costs c - K'y.
 template <typename T>
-__device__ void phase_w(const Args<T> &a, const Control &s, int nb, int rank) {
+__device__ void phase_w(const Args<T> &a, const Control &s, const Team &tm) {
   const T inv = (T)s.inv_w;
   const bool avg = s.w_avg != 0;
   const T *x = a.x[s.xc];
   const T *y = a.y[s.yc];
   int32_t lo, hi;
-  chunk(a.n, nb, rank, lo, hi);
+  chunk(a.n, tm.nb, tm.rank, lo, hi);
   for (int32_t j = lo + threadIdx.x; j < hi; j += kThreads) {
     const T xj = avg ? inv * ldv(a.sx + j) : ldv(x + j);
     const T kt = avg ? inv * ldv(a.skty + j) : ldv(a.kty + j);
@@ -569,32 +601,31 @@ __device__ void phase_w(const Args<T> &a, const Control &s, int nb, int rank) {
     a.xo[j] = (double)xj * cs;
     a.rco[j] = __ldg(a.c0 + j) - (double)kt / cs;
   }
-  chunk(a.m, nb, rank, lo, hi);
+  chunk(a.m, tm.nb, tm.rank, lo, hi);
   for (int32_t r = lo + threadIdx.x; r < hi; r += kThreads) {
     const T yr = avg ? inv * ldv(a.sy + r) : ldv(y + r);
     a.yo[r] = (double)yr * __ldg(a.rs + r);
   }
 }
 
-// ---- decisions (deciding block; `red` is shared) ------------------------------
+// ---- decisions (the whole deciding block; thread 0 updates the record) -------
 
 template <typename T>
-__device__ void decide(const Args<T> &a, Control &c, int phase, int nb, double *red) {
+__device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, double *red) {
   const Params &P = a.P;
   switch (phase) {
     case PH_INIT: {
-      reduce_partials<kMaxQ>(a.partials, a.max_blocks, nb, 0, red);
+      reduce_partials<kMaxQ>(a.partials, a.max_blocks, tm.nb, tm.s_part, red);
       if (threadIdx.x == 0) {
         c.t0 = global_timer_ns();
         const Kkt e = kkt_current(red, P);
-        if (converged(e, P)) {  // Pdhg.scala:211-212
+        c.current = e;
+        if (converged(e, P)) {  // the start is already optimal, Pdhg.scala:211-212
           c.status = PRIMA_STATUS_OPTIMAL;
           c.final_kkt = e;
-          c.current = e;
           c.w_avg = 0;
           c.phase = PH_W;
         } else {
-          c.current = e;
           c.error_at_restart = weighted(e, c.weight);
           c.pend = 0;
           c.trials = 0;
@@ -604,12 +635,8 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, int nb, double *
       }
       break;
     }
-    case PH_A: {
-      if (threadIdx.x == 0) c.phase = PH_B;
-      break;
-    }
     case PH_B: {  // Solve.step's trial decision, Pdhg.scala:336-380
-      reduce_partials<3>(a.partials, a.max_blocks, nb, 0, red);
+      reduce_partials<3>(a.partials, a.max_blocks, tm.nb, tm.s_part, red);
       if (threadIdx.x == 0) {
         c.trials += 1;
         c.total_trials += 1;
@@ -660,7 +687,7 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, int nb, double *
       break;
     }
     case PH_F: {  // checkpoint (Pdhg.scala:396-417) and the terminal evaluations
-      reduce_partials<kMaxQ>(a.partials, a.max_blocks, nb, 0, red);
+      reduce_partials<kMaxQ>(a.partials, a.max_blocks, tm.nb, tm.s_part, red);
       if (threadIdx.x == 0) {
         const Kkt cur = kkt_current(red, P);
         c.current = cur;
@@ -726,7 +753,7 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, int nb, double *
       break;
     }
     case PH_R: {
-      reduce_partials<2>(a.partials, a.max_blocks, nb, 0, red);
+      reduce_partials<2>(a.partials, a.max_blocks, tm.nb, tm.s_part, red);
       if (threadIdx.x == 0) {
         const double pm = sqrt(red[Q_DXR]), dm = sqrt(red[Q_DYR]);
         if (pm > 0.0 && dm > 0.0) {
@@ -746,35 +773,118 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, int nb, double *
       }
       break;
     }
-    case PH_W: {
-      if (threadIdx.x == 0) c.phase = PH_DONE;
-      break;
-    }
-    default:
+    default:  // PH_W
       if (threadIdx.x == 0) c.phase = PH_DONE;
   }
 }
 
+// ---- the team barrier -------------------------------------------------------
+
+constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~seconds; a phase takes microseconds
+
 template <typename T>
-__global__ void __launch_bounds__(kThreads) pdhg_kernel(Args<T> a) {
+__device__ __forceinline__ void publish_control(const Args<T> &a, const Control &snap) {
+  const unsigned *src = (const unsigned *)&snap;
+  unsigned *dst = (unsigned *)a.ctl;
+  for (int i = threadIdx.x; i < (int)(sizeof(Control) / 4); i += kThreads) dst[i] = src[i];
+}
+
+template <typename T>
+__device__ __forceinline__ void load_control(const Args<T> &a, Control &snap) {
+  const unsigned *src = (const unsigned *)a.ctl;
+  unsigned *dst = (unsigned *)&snap;
+  for (int i = threadIdx.x; i < (int)(sizeof(Control) / 4); i += kThreads) dst[i] = __ldcg(src + i);
+  __syncthreads();
+}
+
+// All blocks arrive; the last one reduces, decides and publishes the next
+// Control record, then releases the team.  After phase A nothing needs
+// deciding (B always follows), so that barrier only synchronises.  Every wait
+// is bounded: on timeout the team's abort flag is raised and every block
+// leaves; the host reports PRIMA_ERR_TIMEOUT.  A one-block team synchronises
+// with __syncthreads and keeps its Control in shared memory.
+template <typename T>
+__device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const Team &tm) {
+  __shared__ unsigned s_gen;
+  __shared__ int s_last, s_ok;
+  __shared__ double s_red[kMaxQ];
+  if (tm.nb == 1) {
+    __syncthreads();
+    if (phase == PH_A) {
+      if (threadIdx.x == 0) snap.phase = PH_B;
+    } else {
+      decide<T>(a, snap, phase, tm, s_red);
+    }
+    __syncthreads();
+    return true;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_gen = ld_acquire(&a.sync->gen);
+    const unsigned old = atom_add_acq_rel(&a.sync->count, 1u);
+    s_last = old == (unsigned)(tm.nb - 1);
+    s_ok = 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    if (phase == PH_A) {
+      if (threadIdx.x == 0) snap.phase = PH_B;
+    } else {
+      decide<T>(a, snap, phase, tm, s_red);
+    }
+    __syncthreads();
+    if (phase != PH_A) publish_control(a, snap);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (*((volatile int32_t *)&a.sync->abort)) s_ok = 0;
+      a.sync->count = 0;
+      __threadfence();
+      st_release(&a.sync->gen, s_gen + 1);
+    }
+  } else if (threadIdx.x == 0) {
+    unsigned long long spins = 0;
+    while (ld_acquire(&a.sync->gen) == s_gen) {
+      if (*((volatile int32_t *)&a.sync->abort)) {
+        s_ok = 0;
+        break;
+      }
+      if (++spins > kSpinLimit) {
+        atomicExch(&a.sync->abort, 1);
+        s_ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+    if (phase == PH_A) snap.phase = PH_B;
+  }
+  __syncthreads();
+  if (s_ok && phase != PH_A) load_control(a, snap);
+  return s_ok;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, kMinBlocksPerSm) pdhg_kernel(Args<T> a) {
   __shared__ Control snap;
-  const int nb = gridDim.x, rank = blockIdx.x;
+  __shared__ double s_part[kMaxQ];
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  T *s_prod = reinterpret_cast<T *>(s_dyn);
+  const Team tm{(int)gridDim.x, (int)blockIdx.x, s_part};
   load_control(a, snap);
   for (;;) {
     const int ph = snap.phase;
     if (ph == PH_DONE) break;
     switch (ph) {
-      case PH_INIT: phase_init(a, snap, nb, rank); break;
-      case PH_A: phase_a(a, snap, nb, rank); break;
-      case PH_B: phase_b(a, snap, nb, rank); break;
-      case PH_F: phase_f(a, snap, nb, rank); break;
-      case PH_R: phase_r(a, snap, nb, rank); break;
-      case PH_W: phase_w(a, snap, nb, rank); break;
+      case PH_INIT: phase_init(a, snap, tm, s_prod); break;
+      case PH_A: phase_a(a, snap, tm, s_prod); break;
+      case PH_B: phase_b(a, snap, tm, s_prod); break;
+      case PH_F: phase_f(a, snap, tm, s_prod); break;
+      case PH_R: phase_r(a, snap, tm); break;
+      case PH_W: phase_w(a, snap, tm); break;
       default: break;
     }
-    if (!barrier_decide(a, snap, ph, nb)) break;
-    load_control(a, snap);
+    if (!barrier_decide(a, snap, ph, tm)) break;
   }
+  if (tm.nb == 1) publish_control(a, snap);  // the host reads the final record
 }
 
 }  // namespace dev
@@ -791,7 +901,8 @@ double ms_since(Clock::time_point t) {
   return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
 }
 
-// Bump allocator over the context's solver arena.
+// Bump allocator over the context's solver arena (iterate state only; the
+// problem itself lives in a PreparedLp).
 struct Layout {
   size_t off = 0;
   template <typename U>
@@ -803,99 +914,59 @@ struct Layout {
 };
 
 template <typename T>
-struct SolveBuffers {
-  dev::Args<T> args;
-  size_t bytes = 0;
-  // offsets
-  size_t o_kp, o_kci, o_kv, o_tp, o_tci, o_tv, o_c, o_q, o_l, o_u, o_c0, o_q0, o_l0, o_u0, o_cs, o_rs;
-  size_t o_x[2], o_y[2], o_kx[2], o_xbar, o_kty, o_sx, o_sy, o_skx, o_skty, o_xr, o_yr, o_xo, o_yo, o_rco;
-  size_t o_part, o_ctl, o_sync;
+struct StateLayout {
+  size_t x[2], y[2], kx[2], xbar, kty, sx, sy, skx, skty, xr, yr, xo, yo, rco, part, ctl, sync, bytes;
+  StateLayout(int32_t n, int32_t m, int blocks) {
+    Layout L;
+    for (int i = 0; i < 2; i++) {
+      x[i] = L.take<T>(n);
+      y[i] = L.take<T>(m);
+      kx[i] = L.take<T>(m);
+    }
+    xbar = L.take<T>(n);
+    kty = L.take<T>(n);
+    sx = L.take<T>(n);
+    skty = L.take<T>(n);
+    xr = L.take<T>(n);
+    sy = L.take<T>(m);
+    skx = L.take<T>(m);
+    yr = L.take<T>(m);
+    xo = L.take<double>(n);
+    rco = L.take<double>(n);
+    yo = L.take<double>(m);
+    part = L.take<double>((int64_t)dev::kMaxQ * blocks);
+    ctl = L.take<dev::Control>(1);
+    sync = L.take<dev::Sync>(1);
+    bytes = L.off;
+  }
 };
 
 template <typename T>
-void plan(SolveBuffers<T> &b, int32_t n, int32_t m, int64_t nnz, int max_blocks) {
-  Layout L;
-  b.o_kp = L.take<int32_t>((int64_t)m + 1);
-  b.o_kci = L.take<int32_t>(nnz);
-  b.o_kv = L.take<T>(nnz);
-  b.o_tp = L.take<int32_t>((int64_t)n + 1);
-  b.o_tci = L.take<int32_t>(nnz);
-  b.o_tv = L.take<T>(nnz);
-  b.o_c = L.take<T>(n);
-  b.o_l = L.take<T>(n);
-  b.o_u = L.take<T>(n);
-  b.o_q = L.take<T>(m);
-  b.o_c0 = L.take<double>(n);
-  b.o_l0 = L.take<double>(n);
-  b.o_u0 = L.take<double>(n);
-  b.o_cs = L.take<double>(n);
-  b.o_q0 = L.take<double>(m);
-  b.o_rs = L.take<double>(m);
-  for (int i = 0; i < 2; i++) {
-    b.o_x[i] = L.take<T>(n);
-    b.o_y[i] = L.take<T>(m);
-    b.o_kx[i] = L.take<T>(m);
-  }
-  b.o_xbar = L.take<T>(n);
-  b.o_kty = L.take<T>(n);
-  b.o_sx = L.take<T>(n);
-  b.o_skty = L.take<T>(n);
-  b.o_xr = L.take<T>(n);
-  b.o_sy = L.take<T>(m);
-  b.o_skx = L.take<T>(m);
-  b.o_yr = L.take<T>(m);
-  b.o_xo = L.take<double>(n);
-  b.o_rco = L.take<double>(n);
-  b.o_yo = L.take<double>(m);
-  b.o_part = L.take<double>((int64_t)dev::kMaxQ * max_blocks);
-  b.o_ctl = L.take<dev::Control>(1);
-  b.o_sync = L.take<dev::Sync>(1);
-  b.bytes = L.off;
+constexpr size_t dyn_smem() {
+  return (size_t)dev::kTileCap * sizeof(T);
 }
 
 template <typename T>
-void bind(SolveBuffers<T> &b, char *base, int32_t n, int32_t m, int32_t neq, int max_blocks) {
-  dev::Args<T> &a = b.args;
-  std::memset(&a, 0, sizeof(a));
-  a.n = n;
-  a.m = m;
-  a.neq = neq;
-  a.kp = (const int32_t *)(base + b.o_kp);
-  a.kci = (const int32_t *)(base + b.o_kci);
-  a.kv = (const T *)(base + b.o_kv);
-  a.tp = (const int32_t *)(base + b.o_tp);
-  a.tci = (const int32_t *)(base + b.o_tci);
-  a.tv = (const T *)(base + b.o_tv);
-  a.c = (const T *)(base + b.o_c);
-  a.q = (const T *)(base + b.o_q);
-  a.l = (const T *)(base + b.o_l);
-  a.u = (const T *)(base + b.o_u);
-  a.c0 = (const double *)(base + b.o_c0);
-  a.q0 = (const double *)(base + b.o_q0);
-  a.l0 = (const double *)(base + b.o_l0);
-  a.u0 = (const double *)(base + b.o_u0);
-  a.cs = (const double *)(base + b.o_cs);
-  a.rs = (const double *)(base + b.o_rs);
-  for (int i = 0; i < 2; i++) {
-    a.x[i] = (T *)(base + b.o_x[i]);
-    a.y[i] = (T *)(base + b.o_y[i]);
-    a.kx[i] = (T *)(base + b.o_kx[i]);
+int32_t max_coresident_blocks(Ctx *c, int *out) {
+  int per_sm = 0;
+  PRIMA_CUDA_TRY(cudaFuncSetAttribute(dev::pdhg_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem<T>()));
+  PRIMA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::pdhg_kernel<T>, dev::kThreads, dyn_smem<T>()));
+  if (per_sm < 1) {
+    set_error("solver kernel cannot be resident on an SM");
+    return PRIMA_ERR_CUDA;
   }
-  a.xbar = (T *)(base + b.o_xbar);
-  a.kty = (T *)(base + b.o_kty);
-  a.sx = (T *)(base + b.o_sx);
-  a.sy = (T *)(base + b.o_sy);
-  a.skx = (T *)(base + b.o_skx);
-  a.skty = (T *)(base + b.o_skty);
-  a.xr = (T *)(base + b.o_xr);
-  a.yr = (T *)(base + b.o_yr);
-  a.xo = (double *)(base + b.o_xo);
-  a.yo = (double *)(base + b.o_yo);
-  a.rco = (double *)(base + b.o_rco);
-  a.partials = (double *)(base + b.o_part);
-  a.max_blocks = max_blocks;
-  a.ctl = (dev::Control *)(base + b.o_ctl);
-  a.sync = (dev::Sync *)(base + b.o_sync);
+  *out = per_sm * c->num_sms;
+  return PRIMA_OK;
+}
+
+// Blocks for a solve: small problems (<= 4096 rows and columns) run as one
+// block, whose barriers never leave the SM; anything larger spreads over as
+// many co-resident blocks as have a tile of work (the latency of a tile is
+// hidden by the other blocks on the SM, not by the tile itself).
+inline int team_blocks(int64_t n, int64_t m, int max_blocks) {
+  const int64_t work = std::max<int64_t>(std::max(n, m), 1);
+  if (work <= 4096) return 1;
+  return (int)std::min<int64_t>(max_blocks, (work + dev::kTileRows - 1) / dev::kTileRows);
 }
 
 template <typename T>
@@ -905,15 +976,7 @@ std::vector<T> narrow(const std::vector<double> &v) {
   return out;
 }
 
-template <typename T>
-int32_t h2d(void *dst, const T *src, size_t count, cudaStream_t s) {
-  if (count == 0) return PRIMA_OK;
-  PRIMA_CUDA_TRY(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
-  return PRIMA_OK;
-}
-
 struct SolveRequest {
-  const prima_lp *lp;
   const prima_params *params;
   const prima_warm_start *warm;
   const volatile int32_t *cancel;
@@ -921,86 +984,113 @@ struct SolveRequest {
   prima_solution_info *info;
 };
 
-template <typename T>
-int32_t max_coresident_blocks(Ctx *c, int *out) {
-  int per_sm = 0;
-  PRIMA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::pdhg_kernel<T>, dev::kThreads, 0));
-  if (per_sm < 1) {
-    set_error("solver kernel cannot be resident on an SM");
-    return PRIMA_ERR_CUDA;
-  }
-  *out = per_sm * c->num_sms;
+int32_t check_warm(const PreparedLp &L, const prima_warm_start *w) {
+  if (!w) return PRIMA_OK;
+  if (L.n > 0 && !w->primal) return (set_error("requirement failed: warm start primal is NULL"), PRIMA_ERR_INVALID_ARGUMENT);
+  for (int32_t i = 0; i < L.n; i++)
+    if (!std::isfinite(w->primal[i]))
+      return (set_error("requirement failed: warm start primal vector is not finite"), PRIMA_ERR_INVALID_ARGUMENT);
+  if (L.m > 0 && !w->dual) return (set_error("requirement failed: warm start dual is NULL"), PRIMA_ERR_INVALID_ARGUMENT);
+  for (int32_t r = 0; r < L.m; r++)
+    if (!std::isfinite(w->dual[r]))
+      return (set_error("requirement failed: warm start dual vector is not finite"), PRIMA_ERR_INVALID_ARGUMENT);
   return PRIMA_OK;
 }
 
-// Pdhg.Solve: setup (Solve.<init> + initialise, Pdhg.scala:131-309) on the
-// host, then the whole iteration in one cooperative launch.
+// Pdhg.Solve on a prepared problem: initialise (Pdhg.scala:250-309) on the
+// host -- the opening step, primal weight and the projected start point --
+// then the whole iteration in one cooperative launch.
 template <typename T>
-int32_t solve_on_device(Ctx *c, const SolveRequest &req) {
-  const auto t_start = Clock::now();
-  const prima_lp *lp = req.lp;
+int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::time_point t_start) {
   const prima_params *p = req.params;
   int32_t rc;
-  if ((rc = validate_params(p)) || (rc = validate_lp(lp))) return rc;
-  const int32_t n = lp->num_variables, m = lp->num_constraints, neq = lp->num_equalities;
-  if (req.warm) {
-    if (!req.warm->primal) return (set_error("requirement failed: warm start primal is NULL"), PRIMA_ERR_INVALID_ARGUMENT);
-    for (int32_t i = 0; i < n; i++)
-      if (!std::isfinite(req.warm->primal[i]))
-        return (set_error("requirement failed: warm start primal vector is not finite"), PRIMA_ERR_INVALID_ARGUMENT);
-    if (m > 0 && !req.warm->dual) return (set_error("requirement failed: warm start dual is NULL"), PRIMA_ERR_INVALID_ARGUMENT);
-    for (int32_t r = 0; r < m; r++)
-      if (!std::isfinite(req.warm->dual[r]))
-        return (set_error("requirement failed: warm start dual vector is not finite"), PRIMA_ERR_INVALID_ARGUMENT);
-  }
-  ScaledLp S;
-  prepare_scaled(lp, p, &S);
-  const int64_t nnz = S.K.nnz();
+  if ((rc = check_warm(L, req.warm))) return rc;
+  cudaStream_t s = c->stream;
+  if ((rc = L.materialise<T>(s))) return rc;
+  const int32_t n = L.n, m = L.m, neq = L.neq;
 
-  // initialise (Pdhg.scala:250-309)
-  const double bound = S.scaled_spectral_bound;
+  const double bound = L.scaled_spectral_bound;
   double step = bound > 0.0 ? 1.0 / bound : 1.0;
-  double weight = (S.scaled_c_norm > 0.0 && S.scaled_q_norm > 0.0) ? S.scaled_c_norm / S.scaled_q_norm : 1.0;
+  double weight = (L.scaled_c_norm > 0.0 && L.scaled_q_norm > 0.0) ? L.scaled_c_norm / L.scaled_q_norm : 1.0;
   if (req.warm && !std::isnan(req.warm->step_size)) step = req.warm->step_size;
   if (req.warm && !std::isnan(req.warm->primal_weight)) weight = req.warm->primal_weight;
-  std::vector<double> x0((size_t)n, 0.0), y0((size_t)m, 0.0);
-  if (req.warm)
-    for (int32_t i = 0; i < n; i++) x0[i] = req.warm->primal[i] / S.col_scale[i];
-  for (int32_t i = 0; i < n; i++) {
-    const double lo = S.l[i], hi = S.u[i], v = x0[i];
-    x0[i] = v < lo ? lo : (v > hi ? hi : v);
-  }
-  if (req.warm)
-    for (int32_t r = 0; r < m; r++) {
-      const double v = req.warm->dual[r] / S.row_scale[r];
-      y0[r] = (r >= neq && v < 0.0) ? 0.0 : v;
-    }
 
   int max_blocks = 0;
   if ((rc = max_coresident_blocks<T>(c, &max_blocks))) return rc;
-  const int64_t work = std::max<int64_t>(std::max(n, m), 1);
-  const int blocks = (int)std::min<int64_t>(max_blocks, std::max<int64_t>(1, (work + dev::kThreads - 1) / dev::kThreads));
-
-  SolveBuffers<T> B;
-  plan<T>(B, n, m, nnz, blocks);
-  if ((rc = c->solver_arena.reserve(B.bytes))) return rc;
+  const int blocks = team_blocks(n, m, max_blocks);
+  const StateLayout<T> S(n, m, blocks);
+  if ((rc = c->solver_arena.reserve(S.bytes))) return rc;
   char *base = (char *)c->solver_arena.ptr;
-  bind<T>(B, base, n, m, neq, blocks);
-  cudaStream_t s = c->stream;
 
-  const std::vector<T> kv = narrow<T>(S.K.vals), tv = narrow<T>(S.Kt.vals);
-  const std::vector<T> cc = narrow<T>(S.c), qq = narrow<T>(S.q), ll = narrow<T>(S.l), uu = narrow<T>(S.u);
-  const std::vector<T> xx = narrow<T>(x0), yy = narrow<T>(y0);
-  if ((rc = h2d(base + B.o_kp, S.K.row_ptr.data(), (size_t)m + 1, s)) || (rc = h2d(base + B.o_kci, S.K.col_idx.data(), nnz, s)) ||
-      (rc = h2d(base + B.o_kv, kv.data(), nnz, s)) || (rc = h2d(base + B.o_tp, S.Kt.row_ptr.data(), (size_t)n + 1, s)) ||
-      (rc = h2d(base + B.o_tci, S.Kt.col_idx.data(), nnz, s)) || (rc = h2d(base + B.o_tv, tv.data(), nnz, s)) ||
-      (rc = h2d(base + B.o_c, cc.data(), n, s)) || (rc = h2d(base + B.o_q, qq.data(), m, s)) ||
-      (rc = h2d(base + B.o_l, ll.data(), n, s)) || (rc = h2d(base + B.o_u, uu.data(), n, s)) ||
-      (rc = h2d(base + B.o_c0, lp->objective, n, s)) || (rc = h2d(base + B.o_q0, lp->rhs, m, s)) ||
-      (rc = h2d(base + B.o_l0, lp->lower, n, s)) || (rc = h2d(base + B.o_u0, lp->upper, n, s)) ||
-      (rc = h2d(base + B.o_cs, S.col_scale.data(), n, s)) || (rc = h2d(base + B.o_rs, S.row_scale.data(), m, s)) ||
-      (rc = h2d(base + B.o_x[0], xx.data(), n, s)) || (rc = h2d(base + B.o_y[0], yy.data(), m, s)))
-    return rc;
+  // start point: zero (or the warm start scaled in), projected into the box
+  if (req.warm) {
+    std::vector<double> x0((size_t)n), y0((size_t)m);
+    for (int32_t i = 0; i < n; i++) {
+      const double v = req.warm->primal[i] / L.h_cs[i], lo = L.h_sl[i], hi = L.h_su[i];
+      x0[i] = v < lo ? lo : (v > hi ? hi : v);
+    }
+    for (int32_t r = 0; r < m; r++) {
+      const double v = req.warm->dual[r] / L.h_rs[r];
+      y0[r] = (r >= neq && v < 0.0) ? 0.0 : v;
+    }
+    const std::vector<T> xx = narrow<T>(x0), yy = narrow<T>(y0);
+    if (n) PRIMA_CUDA_TRY(cudaMemcpyAsync(base + S.x[0], xx.data(), (size_t)n * sizeof(T), cudaMemcpyHostToDevice, s));
+    if (m) PRIMA_CUDA_TRY(cudaMemcpyAsync(base + S.y[0], yy.data(), (size_t)m * sizeof(T), cudaMemcpyHostToDevice, s));
+    PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
+  } else {
+    std::vector<double> x0((size_t)n);
+    for (int32_t i = 0; i < n; i++) {
+      const double lo = L.h_sl[i], hi = L.h_su[i];
+      x0[i] = 0.0 < lo ? lo : (0.0 > hi ? hi : 0.0);
+    }
+    const std::vector<T> xx = narrow<T>(x0);
+    if (n) PRIMA_CUDA_TRY(cudaMemcpyAsync(base + S.x[0], xx.data(), (size_t)n * sizeof(T), cudaMemcpyHostToDevice, s));
+    if (m) PRIMA_CUDA_TRY(cudaMemsetAsync(base + S.y[0], 0, (size_t)m * sizeof(T), s));
+    PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+
+  dev::Args<T> a;
+  std::memset(&a, 0, sizeof(a));
+  a.n = n;
+  a.m = m;
+  a.neq = neq;
+  const int w = sizeof(T) == 8 ? 1 : 0;
+  a.kp = L.kp();
+  a.kci = L.kci();
+  a.kv = (const T *)L.copies[w].kv.ptr;
+  a.tp = L.tp();
+  a.tci = L.tci();
+  a.tv = (const T *)L.copies[w].tv.ptr;
+  a.c = (const T *)L.copies[w].c.ptr;
+  a.l = (const T *)L.copies[w].l.ptr;
+  a.u = (const T *)L.copies[w].u.ptr;
+  a.q = (const T *)L.copies[w].q.ptr;
+  a.c0 = L.c0();
+  a.l0 = L.l0();
+  a.u0 = L.u0();
+  a.q0 = L.q0();
+  a.cs = L.cs();
+  a.rs = L.rs();
+  for (int i = 0; i < 2; i++) {
+    a.x[i] = (T *)(base + S.x[i]);
+    a.y[i] = (T *)(base + S.y[i]);
+    a.kx[i] = (T *)(base + S.kx[i]);
+  }
+  a.xbar = (T *)(base + S.xbar);
+  a.kty = (T *)(base + S.kty);
+  a.sx = (T *)(base + S.sx);
+  a.sy = (T *)(base + S.sy);
+  a.skx = (T *)(base + S.skx);
+  a.skty = (T *)(base + S.skty);
+  a.xr = (T *)(base + S.xr);
+  a.yr = (T *)(base + S.yr);
+  a.xo = (double *)(base + S.xo);
+  a.yo = (double *)(base + S.yo);
+  a.rco = (double *)(base + S.rco);
+  a.partials = (double *)(base + S.part);
+  a.max_blocks = blocks;
+  a.ctl = (dev::Control *)(base + S.ctl);
+  a.sync = (dev::Sync *)(base + S.sync);
 
   dev::Control ctl;
   std::memset(&ctl, 0, sizeof(ctl));
@@ -1014,13 +1104,14 @@ int32_t solve_on_device(Ctx *c, const SolveRequest &req) {
   ctl.sigma = step * weight;
   dev::Sync sync;
   std::memset(&sync, 0, sizeof(sync));
-  if ((rc = h2d(base + B.o_ctl, &ctl, 1, s)) || (rc = h2d(base + B.o_sync, &sync, 1, s))) return rc;
+  PRIMA_CUDA_TRY(cudaMemcpyAsync(a.ctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
+  PRIMA_CUDA_TRY(cudaMemcpyAsync(a.sync, &sync, sizeof(sync), cudaMemcpyHostToDevice, s));
 
-  dev::Params &P = B.args.P;
+  dev::Params &P = a.P;
   P.eps_abs = p->eps_abs;
   P.eps_rel = p->eps_rel;
-  P.rhs_norm = S.rhs_norm;
-  P.obj_norm = S.obj_norm;
+  P.rhs_norm = L.rhs_norm;
+  P.obj_norm = L.obj_norm;
   P.max_iterations = p->max_iterations;
   P.eval_freq = p->evaluation_frequency;
   P.time_limit_ms = p->time_limit_ms;
@@ -1029,10 +1120,10 @@ int32_t solve_on_device(Ctx *c, const SolveRequest &req) {
   P.r_nec = p->restart_necessary_reduction;
   P.r_art = p->restart_artificial_fraction;
   P.smoothing = p->primal_weight_smoothing;
-  P.matrix_norm = S.orig_spectral_bound;
-  P.offset = lp->objective_offset;
-  *c->cancel_mapped = (req.cancel && *req.cancel) ? 1 : 0;
-  B.args.cancel = c->cancel_mapped_dev;
+  P.matrix_norm = L.orig_spectral_bound;
+  P.offset = L.host ? L.host->objective_offset : 0.0;
+  *(volatile int32_t *)c->cancel_mapped = (req.cancel && *req.cancel) ? 1 : 0;
+  a.cancel = c->cancel_mapped_dev;
   PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
   const double setup_ms = ms_since(t_start);
   P.setup_ms = setup_ms;
@@ -1040,10 +1131,10 @@ int32_t solve_on_device(Ctx *c, const SolveRequest &req) {
   cudaEvent_t e0, e1;
   PRIMA_CUDA_TRY(cudaEventCreate(&e0));
   PRIMA_CUDA_TRY(cudaEventCreate(&e1));
-  void *kargs[] = {(void *)&B.args};
+  void *kargs[] = {(void *)&a};
   PRIMA_CUDA_TRY(cudaEventRecord(e0, s));
   cudaError_t le = cudaLaunchCooperativeKernel((const void *)dev::pdhg_kernel<T>, dim3(blocks), dim3(dev::kThreads),
-                                               kargs, 0, s);
+                                               kargs, dyn_smem<T>(), s);
   if (le != cudaSuccess) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1051,9 +1142,9 @@ int32_t solve_on_device(Ctx *c, const SolveRequest &req) {
     return PRIMA_ERR_CUDA;
   }
   PRIMA_CUDA_TRY(cudaEventRecord(e1, s));
-  // Wait; while waiting, forward the caller's cancel flag to the mapped flag
-  // the device polls at evaluation points.
-  for (;;) {
+  // Wait; meanwhile forward the caller's cancel flag to the mapped flag the
+  // device polls at evaluation points.
+  for (int spin = 0;; spin++) {
     const cudaError_t q = cudaEventQuery(e1);
     if (q == cudaSuccess) break;
     if (q != cudaErrorNotReady) {
@@ -1061,18 +1152,18 @@ int32_t solve_on_device(Ctx *c, const SolveRequest &req) {
       return PRIMA_ERR_CUDA;
     }
     if (req.cancel && *req.cancel) *(volatile int32_t *)c->cancel_mapped = 1;
-    std::this_thread::sleep_for(std::chrono::microseconds(req.cancel ? 50 : 10));
+    if (spin > 200) std::this_thread::sleep_for(std::chrono::microseconds(20));
   }
   float kms = 0.f;
   cudaEventElapsedTime(&kms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  PRIMA_CUDA_TRY(cudaMemcpy(&ctl, base + B.o_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
-  PRIMA_CUDA_TRY(cudaMemcpy(&sync, base + B.o_sync, sizeof(sync), cudaMemcpyDeviceToHost));
+  PRIMA_CUDA_TRY(cudaMemcpy(&ctl, a.ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+  PRIMA_CUDA_TRY(cudaMemcpy(&sync, a.sync, sizeof(sync), cudaMemcpyDeviceToHost));
   if (sync.abort) ctl.error = PRIMA_ERR_TIMEOUT;
-  if (req.x_out && n) PRIMA_CUDA_TRY(cudaMemcpy(req.x_out, base + B.o_xo, (size_t)n * 8, cudaMemcpyDeviceToHost));
-  if (req.y_out && m) PRIMA_CUDA_TRY(cudaMemcpy(req.y_out, base + B.o_yo, (size_t)m * 8, cudaMemcpyDeviceToHost));
-  if (req.rc_out && n) PRIMA_CUDA_TRY(cudaMemcpy(req.rc_out, base + B.o_rco, (size_t)n * 8, cudaMemcpyDeviceToHost));
+  if (req.x_out && n) PRIMA_CUDA_TRY(cudaMemcpy(req.x_out, a.xo, (size_t)n * 8, cudaMemcpyDeviceToHost));
+  if (req.y_out && m) PRIMA_CUDA_TRY(cudaMemcpy(req.y_out, a.yo, (size_t)m * 8, cudaMemcpyDeviceToHost));
+  if (req.rc_out && n) PRIMA_CUDA_TRY(cudaMemcpy(req.rc_out, a.rco, (size_t)n * 8, cudaMemcpyDeviceToHost));
   prima_solution_info *info = req.info;
   std::memset(info, 0, sizeof(*info));
   info->status = ctl.status;
@@ -1096,9 +1187,136 @@ int32_t solve_on_device(Ctx *c, const SolveRequest &req) {
   return PRIMA_OK;
 }
 
-int32_t dispatch_solve(Ctx *c, const SolveRequest &req, int bits) {
+// Equilibrate (again) if the prepared problem was scaled differently.
+int32_t ensure_prepared(Ctx *c, PreparedLp &L, const prima_lp *lp, const prima_params *p) {
+  if (L.host == lp && L.scaled_like(p)) return PRIMA_OK;
+  const int32_t rc = L.prepare(lp, p, c->stream);
+  L.host = lp;
+  return rc;
+}
+
+int32_t solve_prepared(Ctx *c, PreparedLp &L, const prima_lp *lp, const SolveRequest &req, int bits,
+                       Clock::time_point t0) {
   if (!req.info) return (set_error("requirement failed: info is NULL"), PRIMA_ERR_INVALID_ARGUMENT);
-  return bits == 64 ? solve_on_device<double>(c, req) : solve_on_device<float>(c, req);
+  int32_t rc;
+  if ((rc = validate_params(req.params))) return rc;
+  if ((rc = ensure_prepared(c, L, lp, req.params))) return rc;
+  return bits == 64 ? solve_on_device<double>(c, L, req, t0) : solve_on_device<float>(c, L, req, t0);
+}
+
+// MixedPrecision.solve (MixedPrecision.scala:104-199), reference scheme: a
+// reduced-precision pass on the device (FP32, loosened tolerances), an FP64
+// re-check of any certificate at the caller's tolerance, and an FP64
+// warm-started finish -- also on the device, on the same prepared problem.
+int32_t mixed_two_pass(Ctx *c, PreparedLp &L, const prima_lp *lp, const prima_params *p,
+                       const prima_mixed_params *mp, const volatile int32_t *cancel, double *x_out, double *y_out,
+                       double *rc_out, prima_solution_info *info, prima_mixed_info *minfo, Clock::time_point t0) {
+  const int32_t n = lp->num_variables, m = lp->num_constraints;
+  prima_params rp = *p;
+  rp.eps_abs = std::max(p->eps_abs, mp->reduced_tolerance);
+  rp.eps_rel = std::max(p->eps_rel, mp->reduced_tolerance);
+  rp.max_iterations = std::min(p->max_iterations, mp->reduced_max_iterations);
+  if (p->time_limit_ms >= 0) rp.time_limit_ms = std::max(1.0, std::floor(p->time_limit_ms * mp->reduced_time_share));
+  rp.infeasibility_tolerance = std::max(p->infeasibility_tolerance, mp->reduced_tolerance);
+  std::vector<double> rx((size_t)n), ry((size_t)m), rrc((size_t)n);
+  prima_solution_info rinfo;
+  int32_t rc = solve_prepared(c, L, lp, SolveRequest{&rp, nullptr, cancel, rx.data(), ry.data(), rrc.data(), &rinfo},
+                              32, t0);
+  if (rc) return rc;
+  const int st = rinfo.status;
+  const bool conclusive = st == PRIMA_STATUS_OPTIMAL || st == PRIMA_STATUS_PRIMAL_INFEASIBLE ||
+                          st == PRIMA_STATUS_DUAL_INFEASIBLE;
+  const bool cert_holds = conclusive && st != PRIMA_STATUS_OPTIMAL &&
+                          classify_fp64(lp, rx.data(), ry.data(), p->infeasibility_tolerance) == st;
+  std::memset(minfo, 0, sizeof(*minfo));
+  minfo->reduced_iterations = rinfo.iterations;
+  minfo->reduced_restarts = rinfo.restarts;
+  minfo->reduced_ms = rinfo.solve_ms;
+  if (!mp->always_refine && cert_holds) {
+    *info = rinfo;
+    if (x_out) std::memcpy(x_out, rx.data(), (size_t)n * 8);
+    if (y_out) std::memcpy(y_out, ry.data(), (size_t)m * 8);
+    if (rc_out) std::memcpy(rc_out, rrc.data(), (size_t)n * 8);
+    return PRIMA_OK;
+  }
+  prima_params fp = *p;
+  if (p->time_limit_ms >= 0) fp.time_limit_ms = std::max(1.0, p->time_limit_ms - (double)rinfo.solve_ms);
+  bool usable = true;
+  for (double v : rx) usable = usable && std::isfinite(v);
+  for (double v : ry) usable = usable && std::isfinite(v);
+  prima_warm_start ws;
+  ws.primal = rx.data();
+  ws.dual = ry.data();
+  // WarmStart(solution) keeps the adaptive state only when finite and positive
+  ws.step_size = (std::isfinite(rinfo.final_step_size) && rinfo.final_step_size > 0.0) ? rinfo.final_step_size : NAN;
+  ws.primal_weight =
+      (std::isfinite(rinfo.final_primal_weight) && rinfo.final_primal_weight > 0.0) ? rinfo.final_primal_weight : NAN;
+  const auto t1 = Clock::now();
+  rc = solve_prepared(c, L, lp, SolveRequest{&fp, usable ? &ws : nullptr, cancel, x_out, y_out, rc_out, info}, 64, t1);
+  if (rc) return rc;
+  minfo->refinement_iterations = info->iterations;
+  minfo->refinement_ms = info->solve_ms;
+  minfo->refined = 1;
+  info->device_ms += rinfo.device_ms;
+  info->trials += rinfo.trials;
+  info->solve_ms = (int64_t)ms_since(t0);
+  return PRIMA_OK;
+}
+
+int32_t validate_mixed(const prima_mixed_params *mixed) {
+  if (!mixed) return (set_error("requirement failed: NULL argument"), PRIMA_ERR_INVALID_ARGUMENT);
+  if (!(mixed->reduced_tolerance > 0.0))
+    return (set_error("requirement failed: reducedTolerance must be positive"), PRIMA_ERR_INVALID_ARGUMENT);
+  if (mixed->reduced_max_iterations <= 0)
+    return (set_error("requirement failed: reducedMaxIterations must be positive"), PRIMA_ERR_INVALID_ARGUMENT);
+  if (!(mixed->reduced_time_share > 0.0 && mixed->reduced_time_share < 1.0))
+    return (set_error("requirement failed: reducedTimeShare must lie in (0, 1)"), PRIMA_ERR_INVALID_ARGUMENT);
+  if (mixed->scheme != PRIMA_MIXED_TWO_PASS && mixed->scheme != PRIMA_MIXED_REFINEMENT)
+    return (set_error("requirement failed: unknown mixed-precision scheme"), PRIMA_ERR_INVALID_ARGUMENT);
+  return PRIMA_OK;
+}
+
+int32_t mixed_dispatch(Ctx *c, PreparedLp &L, const prima_lp *lp, const prima_params *params,
+                       const prima_mixed_params *mixed, const volatile int32_t *cancel, double *x_out, double *y_out,
+                       double *rc_out, prima_solution_info *info, prima_mixed_info *minfo, Clock::time_point t0) {
+  int32_t rc;
+  if (!info || !minfo) return (set_error("requirement failed: NULL argument"), PRIMA_ERR_INVALID_ARGUMENT);
+  if ((rc = validate_mixed(mixed)) || (rc = validate_params(params))) return rc;
+  if (c->bits == 64) {
+    // a float64 device skips the reduced pass entirely (MixedPrecision.scala:111-113)
+    rc = solve_prepared(c, L, lp, SolveRequest{params, nullptr, cancel, x_out, y_out, rc_out, info}, 64, t0);
+    if (rc) return rc;
+    std::memset(minfo, 0, sizeof(*minfo));
+    minfo->refinement_iterations = info->iterations;
+    minfo->refinement_ms = info->solve_ms;
+    return PRIMA_OK;
+  }
+  if (mixed->scheme == PRIMA_MIXED_TWO_PASS)
+    return mixed_two_pass(c, L, lp, params, mixed, cancel, x_out, y_out, rc_out, info, minfo, t0);
+  set_error("requirement failed: the refinement scheme is not available in this build");
+  return PRIMA_ERR_INVALID_ARGUMENT;
+}
+
+LpHostCopy *copy_lp(const prima_lp *lp) {
+  auto *h = new LpHostCopy();
+  const int32_t n = lp->num_variables, m = lp->num_constraints;
+  const int64_t nnz = lp->row_ptr[m];
+  h->row_ptr.assign(lp->row_ptr, lp->row_ptr + m + 1);
+  h->col_idx.assign(lp->col_idx, lp->col_idx + nnz);
+  h->values.assign(lp->values, lp->values + nnz);
+  h->objective.assign(lp->objective, lp->objective + n);
+  h->lower.assign(lp->lower, lp->lower + n);
+  h->upper.assign(lp->upper, lp->upper + n);
+  h->rhs.assign(lp->rhs, lp->rhs + m);
+  h->lp = *lp;
+  h->lp.row_ptr = h->row_ptr.data();
+  h->lp.col_idx = h->col_idx.data();
+  h->lp.values = h->values.data();
+  h->lp.objective = h->objective.data();
+  h->lp.lower = h->lower.data();
+  h->lp.upper = h->upper.data();
+  h->lp.rhs = h->rhs.data();
+  return h;
 }
 
 }  // namespace
@@ -1106,40 +1324,90 @@ int32_t dispatch_solve(Ctx *c, const SolveRequest &req, int bits) {
 
 using namespace prima;
 
+#define CTX_OR_RETURN(h)        \
+  clear_error();                \
+  int32_t rc_;                  \
+  Ctx *c = lookup_ctx(h, &rc_); \
+  if (!c) return rc_;           \
+  cudaSetDevice(c->device)
+
 extern "C" int32_t prima_pdhg_solve(prima_handle ctx, const prima_lp *lp, const prima_params *params,
                                     const prima_warm_start *warm, const volatile int32_t *cancel, double *x_out,
                                     double *y_out, double *rc_out, prima_solution_info *info) {
-  clear_error();
+  CTX_OR_RETURN(ctx);
+  const auto t0 = Clock::now();
   int32_t rc;
-  Ctx *c = lookup_ctx(ctx, &rc);
-  if (!c) return rc;
-  cudaSetDevice(c->device);
-  SolveRequest req{lp, params, warm, cancel, x_out, y_out, rc_out, info};
-  return dispatch_solve(c, req, c->bits);
+  if ((rc = validate_lp(lp))) return rc;
+  c->scratch_lp.host = nullptr;  // a one-shot call always re-prepares
+  rc = solve_prepared(c, c->scratch_lp, lp, SolveRequest{params, warm, cancel, x_out, y_out, rc_out, info}, c->bits, t0);
+  c->scratch_lp.host = nullptr;
+  return rc;
 }
 
 extern "C" int32_t prima_mixed_solve(prima_handle ctx, const prima_lp *lp, const prima_params *params,
                                      const prima_mixed_params *mixed, const volatile int32_t *cancel,
                                      double *x_out, double *y_out, double *rc_out, prima_solution_info *info,
                                      prima_mixed_info *minfo) {
-  clear_error();
+  CTX_OR_RETURN(ctx);
+  const auto t0 = Clock::now();
   int32_t rc;
-  Ctx *c = lookup_ctx(ctx, &rc);
-  if (!c) return rc;
-  cudaSetDevice(c->device);
-  set_error("prima_mixed_solve: not built yet");
-  return PRIMA_ERR_INVALID_ARGUMENT;
+  if ((rc = validate_lp(lp))) return rc;
+  c->scratch_lp.host = nullptr;
+  rc = mixed_dispatch(c, c->scratch_lp, lp, params, mixed, cancel, x_out, y_out, rc_out, info, minfo, t0);
+  c->scratch_lp.host = nullptr;
+  return rc;
+}
+
+extern "C" int32_t prima_problem_create(prima_handle ctx, const prima_lp *lp, const prima_params *params,
+                                        prima_handle *problem) {
+  CTX_OR_RETURN(ctx);
+  int32_t rc;
+  if (!problem) return (set_error("requirement failed: output is NULL"), PRIMA_ERR_INVALID_ARGUMENT);
+  if ((rc = validate_lp(lp)) || (rc = validate_params(params))) return rc;
+  auto L = std::make_unique<PreparedLp>();
+  L->owned.reset(copy_lp(lp));
+  if ((rc = ensure_prepared(c, *L, &L->owned->lp, params))) return rc;
+  *problem = c->next_id++;
+  c->problems[*problem] = std::move(L);
+  return PRIMA_OK;
+}
+
+extern "C" int32_t prima_problem_free(prima_handle ctx, prima_handle problem) {
+  CTX_OR_RETURN(ctx);
+  auto it = c->problems.find(problem);
+  if (it == c->problems.end()) return (set_error("unknown problem handle"), PRIMA_ERR_CLOSED);
+  cudaStreamSynchronize(c->stream);
+  c->problems.erase(it);
+  return PRIMA_OK;
+}
+
+extern "C" int32_t prima_problem_solve(prima_handle ctx, prima_handle problem, const prima_params *params,
+                                       const prima_warm_start *warm, const volatile int32_t *cancel, double *x_out,
+                                       double *y_out, double *rc_out, prima_solution_info *info) {
+  CTX_OR_RETURN(ctx);
+  auto it = c->problems.find(problem);
+  if (it == c->problems.end()) return (set_error("unknown problem handle"), PRIMA_ERR_CLOSED);
+  PreparedLp &L = *it->second;
+  return solve_prepared(c, L, &L.owned->lp, SolveRequest{params, warm, cancel, x_out, y_out, rc_out, info}, c->bits,
+                        Clock::now());
+}
+
+extern "C" int32_t prima_problem_mixed_solve(prima_handle ctx, prima_handle problem, const prima_params *params,
+                                             const prima_mixed_params *mixed, const volatile int32_t *cancel,
+                                             double *x_out, double *y_out, double *rc_out, prima_solution_info *info,
+                                             prima_mixed_info *minfo) {
+  CTX_OR_RETURN(ctx);
+  auto it = c->problems.find(problem);
+  if (it == c->problems.end()) return (set_error("unknown problem handle"), PRIMA_ERR_CLOSED);
+  PreparedLp &L = *it->second;
+  return mixed_dispatch(c, L, &L.owned->lp, params, mixed, cancel, x_out, y_out, rc_out, info, minfo, Clock::now());
 }
 
 extern "C" int32_t prima_pdhg_solve_batch(prima_handle ctx, int32_t count, const prima_lp *lps,
                                           const prima_params *params, const volatile int32_t *cancel,
                                           double *const *x_out, double *const *y_out, double *const *rc_out,
                                           prima_solution_info *infos) {
-  clear_error();
-  int32_t rc;
-  Ctx *c = lookup_ctx(ctx, &rc);
-  if (!c) return rc;
-  cudaSetDevice(c->device);
+  CTX_OR_RETURN(ctx);
   set_error("prima_pdhg_solve_batch: not built yet");
   return PRIMA_ERR_INVALID_ARGUMENT;
 }

@@ -40,34 +40,41 @@ namespace dev {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+constexpr int kMinBlocksPerSm = 4;  // register cap 64: enough warps in flight for the gathers
+constexpr int kTileRows = 512;      // rows of one CSR-stream tile (2 per thread)
+constexpr int kRowsPerThread = kTileRows / kThreads;
+constexpr int kTileCap = 4096;      // staged products per tile (dynamic shared memory)
 constexpr int kMaxQ = 17;
 
 enum : int { PH_INIT = 0, PH_A = 1, PH_B = 2, PH_F = 3, PH_R = 4, PH_W = 5, PH_DONE = 6 };
 enum : int { F_FIXPOINT = 0, F_CHECKPOINT = 1, F_ITERLIMIT = 2 };
 
 // Reduction slots.  Trial: A writes DX, B writes DY and INTER.  Evaluation:
-// current-point terms, then average-point terms.  Restart: DXR, DYR.
+// the row terms (slots 0-6) and the column terms (slots 7-16), each reduced
+// right after its loop so at most ten accumulators are live.  Restart: DXR, DYR.
 enum : int { Q_DX = 0, Q_DY = 1, Q_INTER = 2 };
 enum : int {
-  Q_PSQ = 0,   // primal residual^2           (rows)
-  Q_QY,        // q'y                          (rows)
-  Q_YSQ,       // |y|^2                        (rows, primal certificate)
-  Q_CONE,      // dual-cone violation^2        (rows, primal certificate)
-  Q_ROWSQ,     // Kx row violation^2           (rows, dual certificate)
-  Q_CX,        // c'x                          (cols)
-  Q_DTERM,     // bound terms of the dual obj  (cols)
-  Q_DSQ,       // dual residual^2              (cols)
-  Q_PVAL,      // bound terms of the primal certificate value (cols)
-  Q_PRSQ,      // unabsorbed reduced cost^2 of the primal certificate (cols)
-  Q_XSQ,       // |x|^2                        (cols, dual certificate)
-  Q_BSQ,       // bound violation^2            (cols, dual certificate)
-  Q_A_PSQ,     // the same KKT terms for the running average
-  Q_A_QY,
-  Q_A_CX,
+  Q_PSQ = 0,   // primal residual^2                                (rows)
+  Q_QY,        // q'y                                               (rows)
+  Q_YSQ,       // |y|^2, primal certificate                         (rows)
+  Q_CONE,      // dual-cone violation^2, primal certificate         (rows)
+  Q_ROWSQ,     // Kx row violation^2, dual certificate              (rows)
+  Q_A_PSQ,     // primal residual^2 of the running average          (rows)
+  Q_A_QY,      // q'y of the running average                        (rows)
+  Q_CX,        // c'x                                               (cols)
+  Q_DTERM,     // bound terms of the dual objective                 (cols)
+  Q_DSQ,       // dual residual^2                                   (cols)
+  Q_PVAL,      // bound terms of the primal certificate value       (cols)
+  Q_PRSQ,      // unabsorbed reduced cost^2, primal certificate     (cols)
+  Q_XSQ,       // |x|^2, dual certificate                           (cols)
+  Q_BSQ,       // bound violation^2, dual certificate               (cols)
+  Q_A_CX,      // the same KKT terms for the running average        (cols)
   Q_A_DTERM,
   Q_A_DSQ,
   Q_EVAL_N
 };
+constexpr int kRowQ = Q_CX;             // slots [0, 7)
+constexpr int kColQ = Q_EVAL_N - Q_CX;  // slots [7, 17)
 enum : int { Q_DXR = 0, Q_DYR = 1 };
 static_assert(Q_EVAL_N == kMaxQ, "slot count");
 

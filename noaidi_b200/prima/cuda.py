@@ -117,6 +117,12 @@ SIGNATURES = {
                                       _DP, _DP, _DP, C.POINTER(CInfo), C.POINTER(CMixedInfo)]),
     "prima_pdhg_solve_batch": (C.c_int32, [_H, C.c_int32, C.POINTER(CLp), C.POINTER(CParams), _IP,
                                            C.POINTER(_DP), C.POINTER(_DP), C.POINTER(_DP), C.POINTER(CInfo)]),
+    "prima_problem_create": (C.c_int32, [_H, C.POINTER(CLp), C.POINTER(CParams), _HP]),
+    "prima_problem_free": (C.c_int32, [_H, _H]),
+    "prima_problem_solve": (C.c_int32, [_H, _H, C.POINTER(CParams), C.POINTER(CWarm), _IP, _DP, _DP, _DP,
+                                        C.POINTER(CInfo)]),
+    "prima_problem_mixed_solve": (C.c_int32, [_H, _H, C.POINTER(CParams), C.POINTER(CMixedParams), _IP, _DP, _DP,
+                                              _DP, C.POINTER(CInfo), C.POINTER(CMixedInfo)]),
 }
 
 _lib = None
@@ -365,11 +371,15 @@ def to_c_mixed(mixed: MixedPrecisionParams, scheme: int = MIXED_REFINEMENT, max_
                         mixed.reduced_time_share, scheme, max_refinements, refinement_growth)
 
 
+DEFAULT_SCHEME = MIXED_TWO_PASS
+
+
 def mixed_solve(problem: LpProblem, params: PdhgParams = PdhgParams(),
-                mixed: MixedPrecisionParams = MixedPrecisionParams(), scheme: int = MIXED_REFINEMENT,
+                mixed: MixedPrecisionParams = MixedPrecisionParams(), scheme: int = None,
                 cancel: Optional[C.c_int32] = None, device: int = 0, max_refinements: int = 8,
                 refinement_growth: float = 1e4, ctx: Optional[Context] = None) -> MixedPrecisionResult:
     """``MixedPrecision.solve`` with both passes on the GPU."""
+    scheme = DEFAULT_SCHEME if scheme is None else scheme
     ctx = ctx or context(device, 32)
     lpv = _LpView(problem)
     n, m = problem.num_variables, problem.num_constraints
@@ -384,6 +394,60 @@ def mixed_solve(problem: LpProblem, params: PdhgParams = PdhgParams(),
                                int(minfo.reduced_ms), minfo.refinement_iterations, int(minfo.refinement_ms),
                                bool(minfo.refined), minfo.refinement_rounds)
     return res
+
+
+class DeviceProblem:
+    """An LP uploaded and equilibrated once on the device (``prima_problem_*``),
+    then solved any number of times.  ``solve``/``mixed_solve`` with
+    ``want_solution=False`` leave the solution vectors on the device and
+    return only the scalars (status, objective, KKT, iterations)."""
+
+    def __init__(self, problem: LpProblem, params: PdhgParams = PdhgParams(), ctx: Optional[Context] = None,
+                 device: int = 0, precision: int = 64):
+        self.ctx = ctx or context(device, precision)
+        self.problem = problem
+        lpv = _LpView(problem)
+        h = C.c_int64()
+        _check(self.ctx.lib.prima_problem_create(self.ctx.handle, C.byref(lpv.c), C.byref(to_c_params(params)),
+                                                 C.byref(h)))
+        self.handle = h.value
+
+    def _outs(self, want):
+        n, m = self.problem.num_variables, self.problem.num_constraints
+        if want:
+            return np.zeros(n), np.zeros(m), np.zeros(n)
+        return None, None, None
+
+    def solve(self, params: PdhgParams = PdhgParams(), warm_start: Optional[WarmStart] = None,
+              cancel: Optional[C.c_int32] = None, want_solution: bool = True) -> LpSolution:
+        x, y, rc = self._outs(want_solution)
+        warm, keep = _warm(self.problem, warm_start)
+        info = CInfo()
+        _check(self.ctx.lib.prima_problem_solve(self.ctx.handle, self.handle, C.byref(to_c_params(params)),
+                                                None if warm is None else C.byref(warm),
+                                                None if cancel is None else C.cast(C.byref(cancel), _IP), _dp(x),
+                                                _dp(y), _dp(rc), C.byref(info)))
+        return _solution(info, x, y, rc)
+
+    def mixed_solve(self, params: PdhgParams = PdhgParams(), mixed: MixedPrecisionParams = MixedPrecisionParams(),
+                    scheme: int = None, cancel: Optional[C.c_int32] = None, want_solution: bool = True,
+                    max_refinements: int = 8, refinement_growth: float = 1e4) -> MixedPrecisionResult:
+        scheme = DEFAULT_SCHEME if scheme is None else scheme
+        x, y, rc = self._outs(want_solution)
+        info, minfo = CInfo(), CMixedInfo()
+        mp = to_c_mixed(mixed, scheme, max_refinements, refinement_growth)
+        _check(self.ctx.lib.prima_problem_mixed_solve(self.ctx.handle, self.handle, C.byref(to_c_params(params)),
+                                                      C.byref(mp),
+                                                      None if cancel is None else C.cast(C.byref(cancel), _IP),
+                                                      _dp(x), _dp(y), _dp(rc), C.byref(info), C.byref(minfo)))
+        return MixedPrecisionResult(_solution(info, x, y, rc), minfo.reduced_iterations, minfo.reduced_restarts,
+                                    int(minfo.reduced_ms), minfo.refinement_iterations, int(minfo.refinement_ms),
+                                    bool(minfo.refined), minfo.refinement_rounds)
+
+    def free(self) -> None:
+        if self.handle is not None and not self.ctx._closed:
+            _check(self.ctx.lib.prima_problem_free(self.ctx.handle, self.handle))
+        self.handle = None
 
 
 def solve_batch(problems: Sequence[LpProblem], params: PdhgParams = PdhgParams(), precision: int = 64,
