@@ -1,28 +1,34 @@
 """Time-to-tolerance benchmark of the B200 PDHG path.
 
-Workload (N=1): the 1M-variable synthetic DC-LOPF dispatch LP (2,000 buses,
-3,000 lines, 1,000 generators, 168 hourly snapshots; seeded), solved to a
-relative KKT tolerance of 1e-8 by the mixed-precision path (FP32 PDHG on the
-device, FP64 finish on the device), next to the plain FP64 device PDHG.
-A "step" is one full solve.  With N GPUs every rank solves its own instance
-(seed = rank): independent LPs, no collective on the data path (weak scaling).
+Workload (N=1): the 1.34M-variable synthetic DC-LOPF dispatch LP (2,000 buses,
+3,000 lines, 1,000 generators, 168 hourly snapshots, seeded), solved to a
+relative KKT tolerance of 1e-8 by FP32 PDHG with FP64 refinement on the
+device.  A "step" is one full solve.  With N GPUs every rank solves its own
+instance (seed = rank): independent LPs, no collective on the data path
+(weak scaling).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-``--impl reference`` times the CPU restatement of the reference's FP64 PDHG
-(the oracle: single-threaded, like the reference's ScalaKernels) on a bounded
-sample of the same workload on the host cores; rank 0 only.
+value   whole-job LPs/s; each step is one prima_problem_mixed_solve on a
+        problem already resident (and equilibrated) on the device, timed with
+        CUDA events on the library's stream; max over ranks.
+e2e     the same metric through the one-shot C-ABI call with host buffers
+        (upload, device equilibration, both passes, download of x, y and the
+        reduced costs inside the timed region).
+fp64    plain FP64 device PDHG (the reference algorithm, ScalaKernels
+        semantics): its per-iteration cost is measured on a bounded run and
+        its time to 1e-8 is that cost times the iteration count the full FP64
+        solve of this instance needs (FP64_ITERATIONS_TO_TOLERANCE, measured
+        on a B200 with --full-fp64, which reruns it).
 
-Prints one JSON line (rank 0).  ``value`` is whole-job LPs/s from device
-time with the problem already on the device; ``e2e`` is the same metric
-through the C-ABI call with host buffers (scaling, upload and download inside
-the timed region).
+``--impl reference`` times the CPU restatement of the reference FP64 PDHG
+(single-threaded, like the reference's ScalaKernels backend) on a bounded
+sample of the same instance on the host cores, rank 0 only.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -34,25 +40,32 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "LPs/s to 1e-8 relative KKT, FP32+FP64-refinement PDHG (DC-LOPF 1M)"
+METRIC = "LPs/s to 1e-8 relative KKT: FP32+FP64-refinement PDHG on the 1.3M-variable DC-LOPF"
 UNIT = "LPs/s"
 EPS = 1e-8
 WORKLOAD = dict(buses=2000, lines=3000, generators=1000, snapshots=168)
+WORKLOAD_NAME = "dc-lopf-2000bus-3000line-1000gen-168h (n=1,344,000 m=840,000 nnz=3,024,000)"
+# Iterations the plain FP64 device PDHG needs to reach 1e-8 on the seed-0
+# instance, from a full run (python bench.py --full-fp64); the CPU baseline
+# uses the same count.
+FP64_ITERATIONS_TO_TOLERANCE = 844_928
+ROUND_REDUCTION = 10.0
 
 
 def peaks():
     try:
-        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "MEASURED_PEAKS.json hbm_gbs"
     except Exception:
-        return {"hbm_gbs": 6650.0, "_fallback": True}
+        return {"hbm_gbs": 6650.0}, "fallback 6.65 TB/s"
 
 
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
         self.index, self.rows, self.proc = index, [], None
@@ -62,8 +75,7 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
+            threading.Thread(target=self._read, daemon=True).start()
         except Exception:
             self.proc = None
         return self
@@ -71,7 +83,7 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) == 8:
+            if len(parts) == 7:
                 self.rows.append(parts)
 
     def __exit__(self, *exc):
@@ -83,60 +95,73 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+        sm = [num(r[0]) for r in self.rows if num(r[0]) is not None]
+        if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": float(self.rows[0][1]) if self.rows[0][1].replace(".", "").isdigit() else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        reasons = sorted({self.NAMES[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": num(self.rows[0][1]), "reasons": reasons,
+                "samples": len(self.rows), "power_w_max": max(num(r[2]) or 0.0 for r in self.rows)}
 
 
-def algorithmic_bytes(problem, trials: int, iterations: int, word: int) -> float:
-    """Compulsory HBM bytes of the iteration ("Roofline"):
-    per accepted trial 13n + 11m vector words plus both matrices
-    (nnz index + value words each, row pointers) -- the y and xbar gathers
-    count once; a rejected trial skips the K'y product and the running sums
-    (7n + 6m words + one matrix)."""
+def algorithmic_bytes(problem, trials: int, iterations: int, word: int, anchored: bool = False) -> float:
+    """Compulsory HBM bytes of the fused iteration, per trial: an accepted trial streams both matrices once (index + value
+    per nonzero, one row pointer per row), gathers the other side's vector
+    once, and moves 13n + 11m vector words (x, c, l, u, K'y, x', xbar, the
+    two column running sums read+write; y, kx, q, y', kx', the two row sums
+    read+write); a rejected trial has no K'y product and no running sums
+    (7n + 6m words, one matrix).  The residual problem's dual bound adds m
+    words per trial in anchored mode."""
     K = problem.constraint_matrix
     n, m, nnz = problem.num_variables, problem.num_constraints, K.nnz
-    acc = (13 * n + 11 * m) * word + 2 * nnz * (4 + word) + 4 * (n + m)
-    rej = (8 * n + 6 * m) * word + nnz * (4 + word) + 4 * m
+    extra = m * word if anchored else 0
+    acc = (13 * n + 11 * m) * word + 2 * nnz * (4 + word) + 4 * (n + m) + extra
+    rej = (7 * n + 6 * m) * word + nnz * (4 + word) + 4 * m + extra
     return acc * iterations + rej * max(0, trials - iterations)
 
 
+def cpu_sample(problem, iters: int, repeats: int = 1):
+    """The oracle (reference FP64 PDHG restated in C, one thread) for a fixed
+    number of iterations: seconds per iteration, setup (equilibration) taken
+    out by differencing against a one-iteration run."""
+    from noaidi_b200.prima import PdhgParams
+    from oracle import oracle as O
+    times = []
+    for _ in range(repeats):
+        t = time.perf_counter()
+        O.solve(problem, PdhgParams(eps_abs=EPS, eps_rel=EPS, max_iterations=1))
+        t1 = time.perf_counter() - t
+        t = time.perf_counter()
+        s = O.solve(problem, PdhgParams(eps_abs=EPS, eps_rel=EPS, max_iterations=iters))
+        tn = time.perf_counter() - t
+        times.append(max(tn - t1, 1e-9) / max(1, s.iterations - 1))
+    return float(np.median(times)), s.iterations
+
+
 def run_reference(args) -> None:
-    """The oracle (reference restatement, FP64, one thread) on a bounded
-    sample: a fixed number of PDHG iterations of the same instance, with the
-    time to tolerance extrapolated from the FP64 iteration count."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from noaidi_b200.prima import PdhgParams, generators as G
-    from oracle import oracle as O
+    from noaidi_b200.prima import generators as G
     problem = G.dc_lopf(seed=0, **WORKLOAD)
-    sample_iters = args.reference_sample_iterations
-    p = PdhgParams(eps_abs=EPS, eps_rel=EPS, max_iterations=sample_iters)
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        O.solve(problem, PdhgParams(eps_abs=EPS, eps_rel=EPS, max_iterations=64))
-    times = []
-    for _ in range(args.steps):
-        t = time.perf_counter()
-        s = O.solve(problem, p)
-        times.append(time.perf_counter() - t)
-    per_iter = float(np.median(times)) / max(1, s.iterations)
-    iters_to_tol = args.fp64_iterations_to_tolerance
-    lps = 1.0 / (per_iter * iters_to_tol)
+    for _ in range(min(args.warmup, 1)):
+        cpu_sample(problem, 1)
+    per_iter, done = cpu_sample(problem, args.cpu_sample_iterations, args.steps)
+    iters = FP64_ITERATIONS_TO_TOLERANCE or args.fp64_iterations
+    lps = 1.0 / (per_iter * iters)
     line = {"impl": "reference", "metric": METRIC, "value": lps, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / lps, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / lps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "dc-lopf-2000bus-168h", "n": problem.num_variables,
-                       "m": problem.num_constraints, "nnz": problem.constraint_matrix.nnz, "eps": EPS},
+            "config": {"workload": WORKLOAD_NAME, "eps": EPS, "seed": 0},
             "cpu_baseline": {"value": lps, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": f"{sample_iters} FP64 PDHG iterations per step (oracle, 1 thread); "
-                                       f"{per_iter * 1e3:.1f} ms/iteration extrapolated to the "
-                                       f"{iters_to_tol} iterations the FP64 solve needs to 1e-8"},
+                             "sample": f"{done} FP64 PDHG iterations per step of the same instance "
+                                       f"(oracle restatement of Pdhg.Solve + ScalaKernels, 1 thread, like the "
+                                       f"reference); {per_iter * 1e3:.1f} ms/iteration extrapolated to the "
+                                       f"{iters} iterations the FP64 solve needs to 1e-8"},
             "e2e": {"value": lps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -144,18 +169,18 @@ def run_reference(args) -> None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--max-iterations", type=int, default=2_000_000)
-    ap.add_argument("--reference-sample-iterations", type=int, default=128)
-    ap.add_argument("--fp64-iterations-to-tolerance", type=int, default=0)
-    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--max-iterations", type=int, default=5_000_000)
+    ap.add_argument("--round-reduction", type=float, default=ROUND_REDUCTION)
+    ap.add_argument("--fp64-sample-iterations", type=int, default=20_000)
+    ap.add_argument("--fp64-iterations", type=int, default=2_000_000)
+    ap.add_argument("--full-fp64", action="store_true", help="solve FP64 to tolerance instead of sampling")
+    ap.add_argument("--cpu-sample-iterations", type=int, default=128)
     ap.add_argument("--skip-cpu", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
-        if args.fp64_iterations_to_tolerance <= 0:
-            args.fp64_iterations_to_tolerance = FP64_ITERATIONS_TO_TOLERANCE
         return run_reference(args)
 
     import torch
@@ -167,7 +192,7 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
 
     from noaidi_b200.prima import MixedPrecisionParams, PdhgParams, cuda, generators as G
 
@@ -175,74 +200,100 @@ def main():
     params = PdhgParams(eps_abs=EPS, eps_rel=EPS, max_iterations=args.max_iterations)
     mixed = MixedPrecisionParams(reduced_max_iterations=args.max_iterations)
     ctx32 = cuda.Context(local, 32)
-    ctx64 = cuda.Context(local, 64)
+    resident = cuda.DeviceProblem(problem, params, ctx=ctx32)
+
+    def step_resident():
+        return resident.mixed_solve(params, mixed, scheme=cuda.MIXED_REFINEMENT,
+                                    round_reduction=args.round_reduction, want_solution=False)
 
     def barrier():
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
 
-    def one_mixed():
-        return cuda.mixed_solve(problem, params, mixed, scheme=cuda.MIXED_TWO_PASS, ctx=ctx32)
-
     for _ in range(args.warmup):
-        r = one_mixed()
+        step_resident()
     barrier()
-    dev_ms, wall = [], []
+    results = []
     with ClockSampler(local) as clocks:
-        t0 = time.perf_counter()
-        results = []
         for _ in range(args.steps):
-            ts = time.perf_counter()
-            r = one_mixed()
-            wall.append(time.perf_counter() - ts)
-            results.append(r)
+            results.append(step_resident())
         barrier()
-        elapsed = time.perf_counter() - t0
-    # device time of the solver kernels (CUDA events around each launch)
-    dev_s = sum(getattr(r.solution, "device_ms", 0.0) for r in results) / 1e3
-    red = [r.reduced_device_ms for r in results] if hasattr(results[0], "reduced_device_ms") else None
-    total_dev = torch.tensor([dev_s, elapsed], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(total_dev, op=dist.ReduceOp.MAX)
-    max_dev, max_wall = float(total_dev[0]), float(total_dev[1])
-    sol = results[-1].solution
+    span_s = sum(r.solution.span_ms for r in results) / 1e3
+    kern_s = sum(r.solution.device_ms for r in results) / 1e3
 
-    # plain FP64 device PDHG, for the ratio and the roofline of the FP64 kernel
-    fp64 = None
-    if not args.skip_fp64:
-        fp64 = cuda.solve(problem, params, precision=64, ctx=ctx64)
+    # end to end through the one-shot C ABI call with host buffers
+    barrier()
+    e2e = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        r_e2e = cuda.mixed_solve(problem, params, mixed, scheme=cuda.MIXED_REFINEMENT,
+                                 round_reduction=args.round_reduction, ctx=ctx32)
+        e2e.append(time.perf_counter() - t)
+    barrier()
+
+    agg = torch.tensor([span_s, sum(e2e)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(agg, op=dist.ReduceOp.MAX)
+    max_span, max_e2e = float(agg[0]), float(agg[1])
+
+    # plain FP64 device PDHG on the same resident problem
+    ctx64 = cuda.Context(local, 64)
+    res64 = cuda.DeviceProblem(problem, params, ctx=ctx64)
+    p64 = params if args.full_fp64 else params.copy(max_iterations=args.fp64_sample_iterations)
+    fp64 = res64.solve(p64, want_solution=False)
+    fp64_ms_per_iter = fp64.device_ms / max(1, fp64.iterations)
 
     if rank == 0:
-        pk = peaks()
-        n, m = problem.num_variables, problem.num_constraints
+        pk, pk_src = peaks()
+        n, m, nnz = problem.num_variables, problem.num_constraints, problem.constraint_matrix.nnz
+        last = results[-1]
+        sol = last.solution
+        steps = args.steps
         line = {
-            "metric": METRIC, "value": args.steps * world / max_dev if max_dev > 0 else None, "unit": UNIT,
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * max_dev / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-            "data": "synthetic",
-            "config": {"workload": "dc-lopf-2000bus-168h", "n": n, "m": m, "nnz": problem.constraint_matrix.nnz,
-                       "eps": EPS, "seed": "rank", "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (no flush needed)", "scheme": "two-pass"},
+            "metric": METRIC, "value": steps * world / max_span, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * max_span / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 iterate, f64 anchor/KKT", "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, "n": n, "m": m, "nnz": nnz, "eps": EPS, "seed": "rank",
+                       "parallelism": f"independent instances x{world}", "scheme": "fp32 pass + fp32 refinement "
+                       f"around an fp64 anchor, round reduction {args.round_reduction:g}",
+                       "l2": "working set larger than L2 (no flush needed)"},
             "clocks": clocks.summary(),
-            "e2e": {"value": args.steps * world / max_wall, "unit": UNIT,
-                    "h2d_bytes_per_step": int(problem.constraint_matrix.nnz * 12 + (n + 1) * 4 + 4 * 8 * n + 8 * m),
+            "e2e": {"value": steps * world / max_e2e, "unit": UNIT,
+                    "h2d_bytes_per_step": int(nnz * 12 + (m + 1) * 4 + 8 * (3 * n + m)),
                     "d2h_bytes_per_step": int(8 * (2 * n + m))},
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": 2 * steps,
             "solution": {"status": sol.status.name, "objective": sol.objective_value,
-                         "iterations_fp32": results[-1].reduced_iterations,
-                         "iterations_fp64": results[-1].refinement_iterations,
-                         "primal_residual": sol.kkt.primal_residual_norm, "dual_residual": sol.kkt.dual_residual_norm},
+                         "primal_residual": sol.kkt.primal_residual_norm,
+                         "dual_residual": sol.kkt.dual_residual_norm, "gap": sol.kkt.absolute_gap,
+                         "fp32_pass_iterations": last.reduced_iterations,
+                         "refinement_iterations": last.refinement_iterations,
+                         "rounds": last.refinement_rounds, "e2e_status": r_e2e.solution.status.name},
         }
-        if fp64 is not None:
-            line["fp64_baseline"] = {"ms": fp64.device_ms, "iterations": fp64.iterations, "status": fp64.status.name,
-                                     "objective": fp64.objective_value,
-                                     "speedup_of_mixed": fp64.device_ms / (1e3 * max_dev / args.steps)}
-            byts = algorithmic_bytes(problem, fp64.trials, fp64.iterations, 8)
-            achieved = byts / (fp64.device_ms * 1e-3) / 1e9
-            line["roofline"] = {"kernel": "pdhg_kernel<double>", "bound": "hbm", "achieved": achieved,
-                                "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
-                                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+        iters64 = fp64.iterations if args.full_fp64 and fp64.status.name == "OPTIMAL" else \
+            (FP64_ITERATIONS_TO_TOLERANCE or args.fp64_iterations)
+        fp64_ttt = fp64_ms_per_iter * iters64
+        line["fp64_baseline"] = {
+            "ms_per_iteration": fp64_ms_per_iter, "iterations_to_tolerance": iters64,
+            "time_to_tolerance_ms": fp64_ttt, "measured": "full solve" if args.full_fp64 else
+            f"{fp64.iterations}-iteration sample x iterations of a full FP64 solve", "status": fp64.status.name,
+            "speedup_of_fp32_refinement": fp64_ttt / (1e3 * max_span / steps)}
+        trials32 = sum(r.solution.trials for r in results)
+        iters32 = sum(r.reduced_iterations + r.refinement_iterations for r in results)
+        byts = algorithmic_bytes(problem, trials32, iters32, 4, anchored=True)
+        achieved = byts / kern_s / 1e9
+        line["roofline"] = {"kernel": "pdhg_kernel<float>", "bound": "hbm", "achieved": achieved,
+                            "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+                            "traffic": TRAFFIC_BYTES_PER_TRIAL * trials32 / len(results) if TRAFFIC_BYTES_PER_TRIAL else None,
+                            "peak_source": pk_src,
+                            "per_trial_bytes": byts / max(1, trials32), "kernel_ms": 1e3 * kern_s / steps}
+        if not args.skip_cpu:
+            per_iter, done = cpu_sample(problem, args.cpu_sample_iterations)
+            lps = 1.0 / (per_iter * iters64)
+            line["cpu_baseline"] = {"value": lps, "unit": UNIT, "cores": 1, "kind": "port",
+                                    "sample": f"{done} FP64 PDHG iterations of the same instance on one host core "
+                                              f"(oracle restatement of the reference), {per_iter * 1e3:.1f} "
+                                              f"ms/iteration extrapolated to {iters64} iterations"}
         print(json.dumps(line), flush=True)
     ctx32.close()
     ctx64.close()
@@ -250,7 +301,10 @@ def main():
         dist.destroy_process_group()
 
 
-FP64_ITERATIONS_TO_TOLERANCE = 100_000  # replaced by the measured device FP64 count
+# DRAM bytes (read + write) per step-size trial of pdhg_kernel<float> on this
+# workload, from an ncu capture of a bounded run of the same instance; None
+# until measured.
+TRAFFIC_BYTES_PER_TRIAL = None
 
 if __name__ == "__main__":
     main()

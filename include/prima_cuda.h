@@ -163,9 +163,10 @@ typedef struct {
   double dual_residual;
   double final_step_size;
   double final_primal_weight;
-  double device_ms; /* time inside the solver kernels */
+  double device_ms; /* time inside the solver kernels (CUDA events) */
   double setup_ms;  /* scaling, transpose and upload */
   int64_t trials;   /* step-size trials, accepted and rejected */
+  double span_ms;   /* CUDA-event time from the call's first device work to its last */
 } prima_solution_info;
 
 /* Pdhg.solveWith(problem, params, this-context, cancelled, warmStart).
@@ -178,16 +179,23 @@ int32_t prima_pdhg_solve(prima_handle ctx, const prima_lp *lp, const prima_param
                          prima_solution_info *info);
 
 /* MixedPrecision.Params (MixedPrecision.scala:37-79) plus the device scheme. */
-#define PRIMA_MIXED_TWO_PASS 0  /* FP32 pass, FP64 certificate re-check, FP64 warm-started finish */
-#define PRIMA_MIXED_REFINEMENT 1 /* FP32 PDHG on scaled residual LPs, FP64 outer loop */
+/* PRIMA_MIXED_TWO_PASS: the reference scheme -- FP32 pass, FP64 certificate
+ * re-check, FP64 warm-started finish (both passes on the GPU).
+ * PRIMA_MIXED_REFINEMENT: the same FP32 pass, then the finish also in FP32:
+ * PDHG on the residual problem around an FP64 anchor (x*, y*) -- data
+ * c - K'y*, q - Kx*, box [l - x*, u - x*], dual cone y >= -y* -- with the
+ * anchor re-centred at every restart and the KKT test in FP64 on x* + x^. */
+#define PRIMA_MIXED_TWO_PASS 0
+#define PRIMA_MIXED_REFINEMENT 1
 typedef struct {
   double reduced_tolerance;
   int32_t reduced_max_iterations;
   int32_t always_refine;
   double reduced_time_share;
   int32_t scheme;
-  int32_t max_refinements; /* outer rounds of PRIMA_MIXED_REFINEMENT */
-  double refinement_growth; /* cap on the residual rescaling per round */
+  int32_t pad;
+  double round_reduction; /* REFINEMENT: a fresh restart schedule (a new round) opens when
+                             the weighted KKT error has fallen by this factor; 0: never */
 } prima_mixed_params;
 
 void prima_mixed_params_default(prima_mixed_params *p);
@@ -200,7 +208,7 @@ typedef struct {
   int32_t refinement_iterations;
   int32_t refined;
   int64_t refinement_ms;
-  int32_t refinement_rounds;
+  int32_t refinement_rounds; /* REFINEMENT: rounds opened by round_reduction */
   int32_t pad;
 } prima_mixed_info;
 

@@ -44,8 +44,8 @@ extern "C" void prima_mixed_params_default(prima_mixed_params *p) {
   p->always_refine = 0;
   p->reduced_time_share = 0.5;
   p->scheme = PRIMA_MIXED_REFINEMENT;
-  p->max_refinements = 8;
-  p->refinement_growth = 1e4;
+  p->pad = 0;
+  p->round_reduction = 0.0;
 }
 
 namespace prima {

@@ -64,7 +64,7 @@ __device__ __forceinline__ void chunk(int32_t total, int nb, int rank, int32_t &
 // own operands are loaded by `pre` before stage 1, so their latency overlaps
 // the gathers.  A tile with more than kTileCap entries is summed straight
 // from global memory in the same order.
-template <typename T, typename Pre, typename Epi>
+template <typename T, int Cap = kTileCap, typename Pre, typename Epi>
 __device__ __forceinline__ void csr_tiles(int32_t lo, int32_t hi, const int32_t *__restrict__ p,
                                           const int32_t *__restrict__ ci, const T *__restrict__ v, const T *x,
                                           T *s_prod, Pre &&pre, Epi &&epi) {
@@ -84,7 +84,7 @@ __device__ __forceinline__ void csr_tiles(int32_t lo, int32_t hi, const int32_t 
       }
     }
     const int32_t k1 = __ldg(p + r1);
-    const bool staged = (k1 - k0) <= kTileCap;
+    const bool staged = (k1 - k0) <= Cap;
     if (staged) {
 #pragma unroll 4
       for (int32_t k = k0 + threadIdx.x; k < k1; k += kThreads) s_prod[k - k0] = __ldg(v + k) * ldv(x + __ldg(ci + k));
@@ -353,9 +353,69 @@ struct Team {
   double *s_part;  // shared: this block's totals, by slot
 };
 
+// Round-to-+inf / -inf narrowing for the residual problem's bounds, so that
+// anchor + correction never leaves the box or the cone in exact arithmetic.
+template <typename T>
+__device__ __forceinline__ T narrow_up(double v);
+template <typename T>
+__device__ __forceinline__ T narrow_down(double v);
+template <>
+__device__ __forceinline__ float narrow_up<float>(double v) {
+  return __double2float_ru(v);
+}
+template <>
+__device__ __forceinline__ float narrow_down<float>(double v) {
+  return __double2float_rd(v);
+}
+template <>
+__device__ __forceinline__ double narrow_up<double>(double v) {
+  return v;
+}
+template <>
+__device__ __forceinline__ double narrow_down<double>(double v) {
+  return v;
+}
+
+// The anchor's exact products and the residual problem's data (anchored
+// mode): kxa = K xa and ktya = K'ya in FP64, then c - K'ya, q - K xa,
+// l - xa (rounded up), u - xa (rounded down), -ya (rounded up) in T.
+template <typename T>
+__device__ void rebuild_residual_problem(const Args<T> &a, const Team &tm, T *s_prod) {
+  double *s_prod64 = reinterpret_cast<double *>(s_prod);
+  constexpr int kCap64 = (int)(kTileCap * sizeof(T) / sizeof(double));
+  int32_t lo, hi;
+  chunk(a.n, tm.nb, tm.rank, lo, hi);
+  csr_tiles<double, kCap64>(lo, hi, a.tp, a.tci, a.tv64, (const double *)a.ya, s_prod64,
+                            [&](int32_t) { return None{}; }, [&](int32_t j, double kt, None) {
+    a.ktya[j] = kt;
+    const double xa = ldv(a.xa + j);
+    a.cw[j] = (T)(__ldg(a.sc + j) - kt);
+    a.lw[j] = narrow_up<T>(__ldg(a.sl + j) - xa);
+    a.uw[j] = narrow_down<T>(__ldg(a.su + j) - xa);
+  });
+  chunk(a.m, tm.nb, tm.rank, lo, hi);
+  csr_tiles<double, kCap64>(lo, hi, a.kp, a.kci, a.kv64, (const double *)a.xa, s_prod64,
+                            [&](int32_t) { return None{}; }, [&](int32_t r, double kxv, None) {
+    a.kxa[r] = kxv;
+    a.qw[r] = (T)(__ldg(a.sq + r) - kxv);
+    a.ylo[r] = r < a.neq ? T(-CUDART_INF) : narrow_up<T>(-ldv(a.ya + r));
+  });
+}
+
+// The point a (correction) value stands for: anchor + correction in FP64.
+template <typename T>
+__device__ __forceinline__ double at(const double *anchor, int32_t i, T v) {
+  return anchor ? ldv(anchor + i) + (double)v : (double)v;
+}
+
 template <typename T>
 __device__ void phase_init(const Args<T> &a, const Control &s, const Team &tm, T *s_prod) {
   int32_t lo, hi;
+  if (a.anchored) {
+    // the start point is the anchor; the correction starts at zero
+    rebuild_residual_problem(a, tm, s_prod);
+    __syncthreads();
+  }
   {
     double v[kColQ];
 #pragma unroll
@@ -368,7 +428,8 @@ __device__ void phase_init(const Args<T> &a, const Control &s, const Team &tm, T
       a.xr[j] = xj;
       a.sx[j] = T(0);
       a.skty[j] = T(0);
-      eval_col((double)xj, (double)kt, __ldg(a.cs + j), __ldg(a.c0 + j), __ldg(a.l0 + j), __ldg(a.u0 + j), v);
+      eval_col(at(a.xa, j, xj), at(a.ktya, j, kt), __ldg(a.cs + j), __ldg(a.c0 + j), __ldg(a.l0 + j),
+               __ldg(a.u0 + j), v);
     });
     block_partials<kColQ>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_CX, tm.s_part);
   }
@@ -384,7 +445,7 @@ __device__ void phase_init(const Args<T> &a, const Control &s, const Team &tm, T
       a.yr[r] = yv;
       a.sy[r] = T(0);
       a.skx[r] = T(0);
-      eval_row((double)yv, (double)kxv, __ldg(a.rs + r), __ldg(a.q0 + r), r < a.neq, v);
+      eval_row(at(a.ya, r, yv), at(a.kxa, r, kxv), __ldg(a.rs + r), __ldg(a.q0 + r), r < a.neq, v);
     });
     block_partials<kRowQ>(v, a.partials, a.max_blocks, tm.rank, tm.nb, 0, tm.s_part);
   }
@@ -402,8 +463,8 @@ __device__ void phase_a(const Args<T> &a, const Control &s, const Team &tm, T *s
   T *xn_out = a.x[s.xc ^ 1];
   auto step = [&](int32_t j, T xj, T kt) {
     // ScalaKernels.primalStep (:78-98): two-comparison clamp
-    const T st = xj - (tau * (__ldg(a.c + j) - kt));
-    const T lj = __ldg(a.l + j), uj = __ldg(a.u + j);
+    const T st = xj - (tau * (ldv(a.c + j) - kt));
+    const T lj = ldv(a.l + j), uj = ldv(a.u + j);
     const T xn = st < lj ? lj : (st > uj ? uj : st);
     xn_out[j] = xn;
     a.xbar[j] = (T(2) * xn) + (T(-1) * xj);
@@ -445,7 +506,7 @@ __device__ void phase_b(const Args<T> &a, const Control &s, const Team &tm, T *s
   };
   csr_tiles<T>(lo, hi, a.kp, a.kci, a.kv, (const T *)a.xbar, s_prod,
                [&](int32_t r) {
-                 Ops o{ldv(y + r), ldv(kx + r), __ldg(a.q + r), T(0), T(0)};
+                 Ops o{ldv(y + r), ldv(kx + r), ldv(a.q + r), T(0), T(0)};
                  if (pend) {
                    o.sy = ldv(a.sy + r);
                    o.skx = ldv(a.skx + r);
@@ -460,7 +521,10 @@ __device__ void phase_b(const Args<T> &a, const Control &s, const Team &tm, T *s
     }
     // ScalaKernels.dualStep (:100-118)
     T yn = yr + (sigma * (o.q - kb));
-    if (r >= a.neq) yn = yn > T(0) ? yn : T(0);
+    if (r >= a.neq) {  // the cone y >= 0, or y^ >= -ya around an anchor
+      const T lo = a.ylo ? ldv(a.ylo + r) : T(0);
+      yn = yn > lo ? yn : lo;
+    }
     y_out[r] = yn;
     kx_out[r] = (T(0.5) * kb) + (T(0.5) * kxr);
     const T dy = (T(1) * yn) + (T(-1) * yr);
@@ -472,7 +536,7 @@ __device__ void phase_b(const Args<T> &a, const Control &s, const Team &tm, T *s
 }
 
 // Flush the pending commit, optionally refresh kx = K x, evaluate the
-// current point and the running average.
+// current point and the running average (anchor + correction in anchored mode).
 template <typename T>
 __device__ void phase_f(const Args<T> &a, const Control &s, const Team &tm, T *s_prod) {
   const T w = (T)s.pend_w, inv = (T)s.inv_w;
@@ -489,8 +553,9 @@ __device__ void phase_f(const Args<T> &a, const Control &s, const Team &tm, T *s
     auto col = [&](int32_t j, T kt) {
       const T xj = ldv(x + j);
       const double cs = __ldg(a.cs + j), c0 = __ldg(a.c0 + j), l0 = __ldg(a.l0 + j), u0 = __ldg(a.u0 + j);
-      eval_col((double)xj, (double)kt, cs, c0, l0, u0, v);
-      if (avg) eval_col_avg((double)(inv * ldv(a.sx + j)), (double)(inv * ldv(a.skty + j)), cs, c0, l0, u0, v);
+      eval_col(at(a.xa, j, xj), at(a.ktya, j, kt), cs, c0, l0, u0, v);
+      if (avg)
+        eval_col_avg(at(a.xa, j, inv * ldv(a.sx + j)), at(a.ktya, j, inv * ldv(a.skty + j)), cs, c0, l0, u0, v);
     };
     if (pend) {
       csr_tiles<T>(lo, hi, a.tp, a.tci, a.tv, y, s_prod, [&](int32_t) { return None{}; }, [&](int32_t j, T kt, None) {
@@ -513,8 +578,9 @@ __device__ void phase_f(const Args<T> &a, const Control &s, const Team &tm, T *s
     auto row = [&](int32_t r, T kxr) {
       const T yr = ldv(y + r);
       const double rs = __ldg(a.rs + r), q0 = __ldg(a.q0 + r);
-      eval_row((double)yr, (double)kxr, rs, q0, r < a.neq, v);
-      if (avg) eval_row_avg((double)(inv * ldv(a.sy + r)), (double)(inv * ldv(a.skx + r)), rs, q0, r < a.neq, v);
+      eval_row(at(a.ya, r, yr), at(a.kxa, r, kxr), rs, q0, r < a.neq, v);
+      if (avg)
+        eval_row_avg(at(a.ya, r, inv * ldv(a.sy + r)), at(a.kxa, r, inv * ldv(a.skx + r)), rs, q0, r < a.neq, v);
     };
     auto flush = [&](int32_t r) {
       if (pend) {
@@ -539,7 +605,11 @@ __device__ void phase_f(const Args<T> &a, const Control &s, const Team &tm, T *s
 }
 
 // restartAt (Pdhg.scala:478-502): adopt the average if chosen, measure the
-// distance travelled since the last restart, re-centre, reset the sums.
+// distance travelled since the last restart, re-centre, reset the sums.  In
+// anchored mode the restart point is folded into the FP64 anchor (clamped
+// into the box and the cone) and the correction restarts from zero; the
+// distances are the correction's own norms, the last restart point being the
+// anchor itself.
 template <typename T>
 __device__ void phase_r(const Args<T> &a, const Control &s, const Team &tm) {
   double v[2] = {0.0, 0.0};
@@ -561,6 +631,13 @@ __device__ void phase_r(const Args<T> &a, const Control &s, const Team &tm) {
     }
     const T d = (T(1) * xj) + (T(-1) * ldv(a.xr + j));
     v[0] += (double)d * (double)d;
+    if (a.anchored) {
+      const double xn = ldv(a.xa + j) + (double)xj, lb = __ldg(a.sl + j), ub = __ldg(a.su + j);
+      a.xa[j] = xn < lb ? lb : (xn > ub ? ub : xn);
+      x[j] = T(0);
+      a.kty[j] = T(0);
+      xj = T(0);
+    }
     a.xr[j] = xj;
     a.sx[j] = T(0);
     a.skty[j] = T(0);
@@ -577,11 +654,25 @@ __device__ void phase_r(const Args<T> &a, const Control &s, const Team &tm) {
     }
     const T d = (T(1) * yr) + (T(-1) * ldv(a.yr + r));
     v[1] += (double)d * (double)d;
+    if (a.anchored) {
+      const double yn = ldv(a.ya + r) + (double)yr;
+      a.ya[r] = (r >= a.neq && yn < 0.0) ? 0.0 : yn;
+      y[r] = T(0);
+      kx[r] = T(0);
+      yr = T(0);
+    }
     a.yr[r] = yr;
     a.sy[r] = T(0);
     a.skx[r] = T(0);
   }
   block_partials<2>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DXR, tm.s_part);
+}
+
+// Anchored mode, after a re-anchoring: the anchor's exact products and the
+// new residual problem.
+template <typename T>
+__device__ void phase_r2(const Args<T> &a, const Control &s, const Team &tm, T *s_prod) {
+  rebuild_residual_problem(a, tm, s_prod);
 }
 
 // finish (Pdhg.scala:510-532): the evaluated point in the caller's units and
@@ -598,13 +689,13 @@ __device__ void phase_w(const Args<T> &a, const Control &s, const Team &tm) {
     const T xj = avg ? inv * ldv(a.sx + j) : ldv(x + j);
     const T kt = avg ? inv * ldv(a.skty + j) : ldv(a.kty + j);
     const double cs = __ldg(a.cs + j);
-    a.xo[j] = (double)xj * cs;
-    a.rco[j] = __ldg(a.c0 + j) - (double)kt / cs;
+    a.xo[j] = at(a.xa, j, xj) * cs;
+    a.rco[j] = __ldg(a.c0 + j) - at(a.ktya, j, kt) / cs;
   }
   chunk(a.m, tm.nb, tm.rank, lo, hi);
   for (int32_t r = lo + threadIdx.x; r < hi; r += kThreads) {
     const T yr = avg ? inv * ldv(a.sy + r) : ldv(y + r);
-    a.yo[r] = (double)yr * __ldg(a.rs + r);
+    a.yo[r] = at(a.ya, r, yr) * __ldg(a.rs + r);
   }
 }
 
@@ -627,6 +718,7 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
           c.phase = PH_W;
         } else {
           c.error_at_restart = weighted(e, c.weight);
+          c.round_err = c.error_at_restart;
           c.pend = 0;
           c.trials = 0;
           set_trial_scalars(c);
@@ -652,7 +744,7 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
         } else {
           const double interaction = fabs(red[Q_INTER]);
           const double limit = interaction > 0.0 ? movement / interaction : CUDART_INF;
-          const double t = (double)(c.iteration + 1);
+          const double t = (double)(c.iteration - c.period_base + 1);
           const double by_rule = (1.0 - pow(t, -0.3)) * limit;
           const double by_cap = (1.0 + pow(t, -0.6)) * c.step;
           const double proposed = dmin(by_rule, by_cap);
@@ -737,11 +829,17 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
               // shouldRestart, Pdhg.scala:463-469
               const bool sufficient = cand <= P.r_suff * c.error_at_restart;
               const bool necessary = cand <= P.r_nec * c.error_at_restart && cand > c.last_candidate;
-              const bool artificial =
-                  (double)(c.iteration - c.last_restart_it) >= P.r_art * (double)c.iteration;
-              if (sufficient || necessary || artificial) {
+              const bool artificial = (double)(c.iteration - c.last_restart_it) >=
+                                      P.r_art * (double)(c.iteration - c.period_base);
+              const bool new_round = P.round_rho > 0.0 && cand <= P.round_rho * c.round_err;
+              if (sufficient || necessary || artificial || new_round) {
                 c.r_avg = use_avg;
                 c.phase = PH_R;
+                if (new_round) {  // fresh restart schedule and step-size ramp
+                  c.period_base = c.iteration;
+                  c.round_err = cand;
+                  c.rounds += 1;
+                }
               } else {
                 c.last_candidate = cand;
                 after_checkpoint(c, cur, P, a.cancel);
@@ -769,8 +867,16 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
         c.error_at_restart = weighted(point, c.weight);
         c.last_candidate = CUDART_INF;
         set_trial_scalars(c);
-        after_checkpoint(c, point, P, a.cancel);
+        if (a.anchored) {
+          c.phase = PH_R2;  // rebuild the residual problem around the new anchor
+        } else {
+          after_checkpoint(c, point, P, a.cancel);
+        }
       }
+      break;
+    }
+    case PH_R2: {
+      if (threadIdx.x == 0) after_checkpoint(c, c.current, P, a.cancel);
       break;
     }
     default:  // PH_W
@@ -880,6 +986,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksPerSm) pdhg_kernel(Args<T>
       case PH_F: phase_f(a, snap, tm, s_prod); break;
       case PH_R: phase_r(a, snap, tm); break;
       case PH_W: phase_w(a, snap, tm); break;
+      case PH_R2: phase_r2(a, snap, tm, s_prod); break;
       default: break;
     }
     if (!barrier_decide(a, snap, ph, tm)) break;
@@ -916,8 +1023,20 @@ struct Layout {
 template <typename T>
 struct StateLayout {
   size_t x[2], y[2], kx[2], xbar, kty, sx, sy, skx, skty, xr, yr, xo, yo, rco, part, ctl, sync, bytes;
-  StateLayout(int32_t n, int32_t m, int blocks) {
+  size_t xa = 0, ya = 0, kxa = 0, ktya = 0, cw = 0, lw = 0, uw = 0, qw = 0, ylo = 0;
+  StateLayout(int32_t n, int32_t m, int blocks, bool anchored) {
     Layout L;
+    if (anchored) {
+      xa = L.take<double>(n);
+      ktya = L.take<double>(n);
+      ya = L.take<double>(m);
+      kxa = L.take<double>(m);
+      cw = L.take<T>(n);
+      lw = L.take<T>(n);
+      uw = L.take<T>(n);
+      qw = L.take<T>(m);
+      ylo = L.take<T>(m);
+    }
     for (int i = 0; i < 2; i++) {
       x[i] = L.take<T>(n);
       y[i] = L.take<T>(m);
@@ -982,6 +1101,9 @@ struct SolveRequest {
   const volatile int32_t *cancel;
   double *x_out, *y_out, *rc_out;
   prima_solution_info *info;
+  bool anchored = false;    // iterate on the residual problem around an FP64 anchor
+  double round_rho = 0.0;   // anchored: error reduction that opens a new round (0: never)
+  int32_t *rounds = nullptr;
 };
 
 int32_t check_warm(const PreparedLp &L, const prima_warm_start *w) {
@@ -1018,34 +1140,39 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   int max_blocks = 0;
   if ((rc = max_coresident_blocks<T>(c, &max_blocks))) return rc;
   const int blocks = team_blocks(n, m, max_blocks);
-  const StateLayout<T> S(n, m, blocks);
+  const bool anchored = req.anchored;
+  if (anchored && (rc = L.materialise<double>(s))) return rc;
+  const StateLayout<T> S(n, m, blocks, anchored);
   if ((rc = c->solver_arena.reserve(S.bytes))) return rc;
   char *base = (char *)c->solver_arena.ptr;
 
-  // start point: zero (or the warm start scaled in), projected into the box
-  if (req.warm) {
-    std::vector<double> x0((size_t)n), y0((size_t)m);
+  // start point: zero (or the warm start scaled in), projected into the box;
+  // in anchored mode it becomes the FP64 anchor and the correction is zero
+  {
+    std::vector<double> x0((size_t)n, 0.0), y0((size_t)m, 0.0);
     for (int32_t i = 0; i < n; i++) {
-      const double v = req.warm->primal[i] / L.h_cs[i], lo = L.h_sl[i], hi = L.h_su[i];
+      const double v = req.warm ? req.warm->primal[i] / L.h_cs[i] : 0.0, lo = L.h_sl[i], hi = L.h_su[i];
       x0[i] = v < lo ? lo : (v > hi ? hi : v);
     }
-    for (int32_t r = 0; r < m; r++) {
-      const double v = req.warm->dual[r] / L.h_rs[r];
-      y0[r] = (r >= neq && v < 0.0) ? 0.0 : v;
+    if (req.warm)
+      for (int32_t r = 0; r < m; r++) {
+        const double v = req.warm->dual[r] / L.h_rs[r];
+        y0[r] = (r >= neq && v < 0.0) ? 0.0 : v;
+      }
+    if (anchored) {
+      if (n) {
+        PRIMA_CUDA_TRY(cudaMemcpyAsync(base + S.xa, x0.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s));
+        PRIMA_CUDA_TRY(cudaMemsetAsync(base + S.x[0], 0, (size_t)n * sizeof(T), s));
+      }
+      if (m) {
+        PRIMA_CUDA_TRY(cudaMemcpyAsync(base + S.ya, y0.data(), (size_t)m * 8, cudaMemcpyHostToDevice, s));
+        PRIMA_CUDA_TRY(cudaMemsetAsync(base + S.y[0], 0, (size_t)m * sizeof(T), s));
+      }
+    } else {
+      const std::vector<T> xx = narrow<T>(x0), yy = narrow<T>(y0);
+      if (n) PRIMA_CUDA_TRY(cudaMemcpyAsync(base + S.x[0], xx.data(), (size_t)n * sizeof(T), cudaMemcpyHostToDevice, s));
+      if (m) PRIMA_CUDA_TRY(cudaMemcpyAsync(base + S.y[0], yy.data(), (size_t)m * sizeof(T), cudaMemcpyHostToDevice, s));
     }
-    const std::vector<T> xx = narrow<T>(x0), yy = narrow<T>(y0);
-    if (n) PRIMA_CUDA_TRY(cudaMemcpyAsync(base + S.x[0], xx.data(), (size_t)n * sizeof(T), cudaMemcpyHostToDevice, s));
-    if (m) PRIMA_CUDA_TRY(cudaMemcpyAsync(base + S.y[0], yy.data(), (size_t)m * sizeof(T), cudaMemcpyHostToDevice, s));
-    PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
-  } else {
-    std::vector<double> x0((size_t)n);
-    for (int32_t i = 0; i < n; i++) {
-      const double lo = L.h_sl[i], hi = L.h_su[i];
-      x0[i] = 0.0 < lo ? lo : (0.0 > hi ? hi : 0.0);
-    }
-    const std::vector<T> xx = narrow<T>(x0);
-    if (n) PRIMA_CUDA_TRY(cudaMemcpyAsync(base + S.x[0], xx.data(), (size_t)n * sizeof(T), cudaMemcpyHostToDevice, s));
-    if (m) PRIMA_CUDA_TRY(cudaMemsetAsync(base + S.y[0], 0, (size_t)m * sizeof(T), s));
     PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
   }
 
@@ -1091,6 +1218,28 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   a.max_blocks = blocks;
   a.ctl = (dev::Control *)(base + S.ctl);
   a.sync = (dev::Sync *)(base + S.sync);
+  if (anchored) {
+    a.anchored = 1;
+    a.xa = (double *)(base + S.xa);
+    a.ya = (double *)(base + S.ya);
+    a.kxa = (double *)(base + S.kxa);
+    a.ktya = (double *)(base + S.ktya);
+    a.sc = L.sc();
+    a.sq = L.sq();
+    a.sl = L.sl();
+    a.su = L.su();
+    a.kv64 = (const double *)L.copies[1].kv.ptr;
+    a.tv64 = (const double *)L.copies[1].tv.ptr;
+    a.cw = (T *)(base + S.cw);
+    a.lw = (T *)(base + S.lw);
+    a.uw = (T *)(base + S.uw);
+    a.qw = (T *)(base + S.qw);
+    a.ylo = (T *)(base + S.ylo);
+    a.c = a.cw;
+    a.l = a.lw;
+    a.u = a.uw;
+    a.q = a.qw;
+  }
 
   dev::Control ctl;
   std::memset(&ctl, 0, sizeof(ctl));
@@ -1122,6 +1271,7 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   P.smoothing = p->primal_weight_smoothing;
   P.matrix_norm = L.orig_spectral_bound;
   P.offset = L.host ? L.host->objective_offset : 0.0;
+  P.round_rho = anchored ? req.round_rho : 0.0;
   *(volatile int32_t *)c->cancel_mapped = (req.cancel && *req.cancel) ? 1 : 0;
   a.cancel = c->cancel_mapped_dev;
   PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1180,6 +1330,7 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   info->setup_ms = setup_ms;
   info->trials = ctl.total_trials;
   info->solve_ms = (int64_t)ms_since(t_start);
+  if (req.rounds) *req.rounds = ctl.rounds;
   if (ctl.error) {
     set_error("a bounded device-side wait gave up; the solve was abandoned");
     return PRIMA_ERR_TIMEOUT;
@@ -1208,9 +1359,20 @@ int32_t solve_prepared(Ctx *c, PreparedLp &L, const prima_lp *lp, const SolveReq
 // reduced-precision pass on the device (FP32, loosened tolerances), an FP64
 // re-check of any certificate at the caller's tolerance, and an FP64
 // warm-started finish -- also on the device, on the same prepared problem.
-int32_t mixed_two_pass(Ctx *c, PreparedLp &L, const prima_lp *lp, const prima_params *p,
-                       const prima_mixed_params *mp, const volatile int32_t *cancel, double *x_out, double *y_out,
-                       double *rc_out, prima_solution_info *info, prima_mixed_info *minfo, Clock::time_point t0) {
+//
+// REFINEMENT scheme: the same reduced pass and certificate re-check, then the
+// finish in FP32 too -- PDHG on the residual problem around an FP64 anchor
+// placed at the reduced pass's answer (step size and primal weight carried),
+// with the anchor re-centred at every restart and convergence judged in FP64
+// on anchor + correction.  Each restart period only has to gain about a
+// decade, far inside FP32's precision, so the FP32 iterations reach any
+// tolerance FP64 could.  A Farkas ray is another matter: certifying
+// infeasibility to a tight tolerance needs the diverging iterate itself to
+// 1e-8 or better, beyond an FP32 correction's rounding, so when the reduced
+// pass did not end Optimal the finish stays in FP64, as in the reference.
+int32_t mixed_passes(Ctx *c, PreparedLp &L, const prima_lp *lp, const prima_params *p,
+                     const prima_mixed_params *mp, const volatile int32_t *cancel, double *x_out, double *y_out,
+                     double *rc_out, prima_solution_info *info, prima_mixed_info *minfo, Clock::time_point t0) {
   const int32_t n = lp->num_variables, m = lp->num_constraints;
   prima_params rp = *p;
   rp.eps_abs = std::max(p->eps_abs, mp->reduced_tolerance);
@@ -1252,7 +1414,15 @@ int32_t mixed_two_pass(Ctx *c, PreparedLp &L, const prima_lp *lp, const prima_pa
   ws.primal_weight =
       (std::isfinite(rinfo.final_primal_weight) && rinfo.final_primal_weight > 0.0) ? rinfo.final_primal_weight : NAN;
   const auto t1 = Clock::now();
-  rc = solve_prepared(c, L, lp, SolveRequest{&fp, usable ? &ws : nullptr, cancel, x_out, y_out, rc_out, info}, 64, t1);
+  SolveRequest finish{&fp, usable ? &ws : nullptr, cancel, x_out, y_out, rc_out, info};
+  if (mp->scheme == PRIMA_MIXED_REFINEMENT && st == PRIMA_STATUS_OPTIMAL) {
+    finish.anchored = true;
+    finish.round_rho = mp->round_reduction > 0.0 ? 1.0 / mp->round_reduction : 0.0;
+    finish.rounds = &minfo->refinement_rounds;
+    rc = solve_prepared(c, L, lp, finish, 32, t1);
+  } else {
+    rc = solve_prepared(c, L, lp, finish, 64, t1);
+  }
   if (rc) return rc;
   minfo->refinement_iterations = info->iterations;
   minfo->refinement_ms = info->solve_ms;
@@ -1273,6 +1443,8 @@ int32_t validate_mixed(const prima_mixed_params *mixed) {
     return (set_error("requirement failed: reducedTimeShare must lie in (0, 1)"), PRIMA_ERR_INVALID_ARGUMENT);
   if (mixed->scheme != PRIMA_MIXED_TWO_PASS && mixed->scheme != PRIMA_MIXED_REFINEMENT)
     return (set_error("requirement failed: unknown mixed-precision scheme"), PRIMA_ERR_INVALID_ARGUMENT);
+  if (!(mixed->round_reduction == 0.0 || mixed->round_reduction > 1.0))
+    return (set_error("requirement failed: roundReduction must be 0 (off) or greater than 1"), PRIMA_ERR_INVALID_ARGUMENT);
   return PRIMA_OK;
 }
 
@@ -1291,11 +1463,27 @@ int32_t mixed_dispatch(Ctx *c, PreparedLp &L, const prima_lp *lp, const prima_pa
     minfo->refinement_ms = info->solve_ms;
     return PRIMA_OK;
   }
-  if (mixed->scheme == PRIMA_MIXED_TWO_PASS)
-    return mixed_two_pass(c, L, lp, params, mixed, cancel, x_out, y_out, rc_out, info, minfo, t0);
-  set_error("requirement failed: the refinement scheme is not available in this build");
-  return PRIMA_ERR_INVALID_ARGUMENT;
+  return mixed_passes(c, L, lp, params, mixed, cancel, x_out, y_out, rc_out, info, minfo, t0);
 }
+
+// CUDA events on the context stream bracketing a whole coarse call.
+struct Span {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  explicit Span(cudaStream_t st) : s(st) {
+    if (cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess) cudaEventRecord(a, s);
+  }
+  double stop() {
+    float ms = 0.f;
+    if (a && b && cudaEventRecord(b, s) == cudaSuccess && cudaEventSynchronize(b) == cudaSuccess)
+      cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  }
+  ~Span() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
 
 LpHostCopy *copy_lp(const prima_lp *lp) {
   auto *h = new LpHostCopy();
@@ -1339,8 +1527,10 @@ extern "C" int32_t prima_pdhg_solve(prima_handle ctx, const prima_lp *lp, const 
   int32_t rc;
   if ((rc = validate_lp(lp))) return rc;
   c->scratch_lp.host = nullptr;  // a one-shot call always re-prepares
+  Span span(c->stream);
   rc = solve_prepared(c, c->scratch_lp, lp, SolveRequest{params, warm, cancel, x_out, y_out, rc_out, info}, c->bits, t0);
   c->scratch_lp.host = nullptr;
+  if (!rc) info->span_ms = span.stop();
   return rc;
 }
 
@@ -1353,8 +1543,10 @@ extern "C" int32_t prima_mixed_solve(prima_handle ctx, const prima_lp *lp, const
   int32_t rc;
   if ((rc = validate_lp(lp))) return rc;
   c->scratch_lp.host = nullptr;
+  Span span(c->stream);
   rc = mixed_dispatch(c, c->scratch_lp, lp, params, mixed, cancel, x_out, y_out, rc_out, info, minfo, t0);
   c->scratch_lp.host = nullptr;
+  if (!rc) info->span_ms = span.stop();
   return rc;
 }
 
@@ -1388,8 +1580,11 @@ extern "C" int32_t prima_problem_solve(prima_handle ctx, prima_handle problem, c
   auto it = c->problems.find(problem);
   if (it == c->problems.end()) return (set_error("unknown problem handle"), PRIMA_ERR_CLOSED);
   PreparedLp &L = *it->second;
-  return solve_prepared(c, L, &L.owned->lp, SolveRequest{params, warm, cancel, x_out, y_out, rc_out, info}, c->bits,
-                        Clock::now());
+  Span span(c->stream);
+  const int32_t rc = solve_prepared(c, L, &L.owned->lp, SolveRequest{params, warm, cancel, x_out, y_out, rc_out, info},
+                                    c->bits, Clock::now());
+  if (!rc) info->span_ms = span.stop();
+  return rc;
 }
 
 extern "C" int32_t prima_problem_mixed_solve(prima_handle ctx, prima_handle problem, const prima_params *params,
@@ -1400,7 +1595,11 @@ extern "C" int32_t prima_problem_mixed_solve(prima_handle ctx, prima_handle prob
   auto it = c->problems.find(problem);
   if (it == c->problems.end()) return (set_error("unknown problem handle"), PRIMA_ERR_CLOSED);
   PreparedLp &L = *it->second;
-  return mixed_dispatch(c, L, &L.owned->lp, params, mixed, cancel, x_out, y_out, rc_out, info, minfo, Clock::now());
+  Span span(c->stream);
+  const int32_t rc = mixed_dispatch(c, L, &L.owned->lp, params, mixed, cancel, x_out, y_out, rc_out, info, minfo,
+                                    Clock::now());
+  if (!rc) info->span_ms = span.stop();
+  return rc;
 }
 
 extern "C" int32_t prima_pdhg_solve_batch(prima_handle ctx, int32_t count, const prima_lp *lps,

@@ -46,7 +46,7 @@ constexpr int kRowsPerThread = kTileRows / kThreads;
 constexpr int kTileCap = 4096;      // staged products per tile (dynamic shared memory)
 constexpr int kMaxQ = 17;
 
-enum : int { PH_INIT = 0, PH_A = 1, PH_B = 2, PH_F = 3, PH_R = 4, PH_W = 5, PH_DONE = 6 };
+enum : int { PH_INIT = 0, PH_A = 1, PH_B = 2, PH_F = 3, PH_R = 4, PH_W = 5, PH_DONE = 6, PH_R2 = 7 };
 enum : int { F_FIXPOINT = 0, F_CHECKPOINT = 1, F_ITERLIMIT = 2 };
 
 // Reduction slots.  Trial: A writes DX, B writes DY and INTER.  Evaluation:
@@ -89,6 +89,7 @@ struct Params {
   double infeas_tol, r_suff, r_nec, r_art, smoothing;
   double matrix_norm;  // spectral bound of the ORIGINAL matrix (certificates)
   double offset;
+  double round_rho;  // anchored mode: a checkpoint this far below the round's start error opens a new round
 };
 
 // Published by the deciding block at every barrier.
@@ -96,12 +97,13 @@ struct Control {
   int32_t phase, f_mode, f_avg, r_avg;
   int32_t w_avg, pend, xc, yc;
   int32_t kxc, status, iteration, restarts;
-  int32_t last_restart_it, trials, error, pad;
+  int32_t last_restart_it, trials, error, period_base;
   int64_t total_trials;
   uint64_t t0;
   double step, weight, weight_sum, pend_w;
   double inv_w, tau, sigma, error_at_restart;
-  double last_candidate, pad2;
+  double last_candidate, round_err;
+  int32_t rounds, pad3;
   Kkt current, average, final_kkt;
 };
 
@@ -130,7 +132,16 @@ struct Args {
   // solution in the caller's units
   double *xo, *yo, *rco;
   double *partials;  // [kMaxQ][max_blocks]
-  int32_t max_blocks, pad2;
+  int32_t max_blocks, anchored;
+  // Anchored (refinement) mode: the iterate is a correction (x^, y^) to an
+  // FP64 anchor (xa, ya) whose exact products kxa = K xa, ktya = K'ya are
+  // kept; the working data c, q, l, u, ylo are the residual problem
+  // (c - K'ya, q - K xa, l - xa, u - xa, -ya) in T, rebuilt at every
+  // re-anchoring.  nullptr in the plain mode.
+  double *xa, *ya, *kxa, *ktya;
+  const double *sc, *sq, *sl, *su;  // FP64 equilibrated data
+  const double *kv64, *tv64;        // FP64 equilibrated matrix values
+  T *cw, *qw, *lw, *uw, *ylo;       // the residual problem's data
   Control *ctl;
   Sync *sync;
   const volatile int32_t *cancel;

@@ -69,13 +69,13 @@ class CInfo(C.Structure):
                 ("device_error", C.c_int32), ("solve_ms", C.c_int64), ("objective", C.c_double),
                 ("dual_objective", C.c_double), ("primal_residual", C.c_double), ("dual_residual", C.c_double),
                 ("final_step_size", C.c_double), ("final_primal_weight", C.c_double), ("device_ms", C.c_double),
-                ("setup_ms", C.c_double), ("trials", C.c_int64)]
+                ("setup_ms", C.c_double), ("trials", C.c_int64), ("span_ms", C.c_double)]
 
 
 class CMixedParams(C.Structure):
     _fields_ = [("reduced_tolerance", C.c_double), ("reduced_max_iterations", C.c_int32),
                 ("always_refine", C.c_int32), ("reduced_time_share", C.c_double), ("scheme", C.c_int32),
-                ("max_refinements", C.c_int32), ("refinement_growth", C.c_double)]
+                ("pad", C.c_int32), ("round_reduction", C.c_double)]
 
 
 class CMixedInfo(C.Structure):
@@ -315,6 +315,7 @@ def _solution(info: CInfo, x, y, rc) -> LpSolution:
     sol.device_ms = info.device_ms
     sol.setup_ms = info.setup_ms
     sol.trials = info.trials
+    sol.span_ms = info.span_ms
     return sol
 
 
@@ -365,19 +366,18 @@ def solve(problem: LpProblem, params: PdhgParams = PdhgParams(), precision: int 
     return _solution(info, x, y, rc)
 
 
-def to_c_mixed(mixed: MixedPrecisionParams, scheme: int = MIXED_REFINEMENT, max_refinements: int = 8,
-               refinement_growth: float = 1e4) -> CMixedParams:
+def to_c_mixed(mixed: MixedPrecisionParams, scheme: int = MIXED_REFINEMENT, round_reduction: float = 0.0) -> CMixedParams:
     return CMixedParams(mixed.reduced_tolerance, mixed.reduced_max_iterations, int(mixed.always_refine),
-                        mixed.reduced_time_share, scheme, max_refinements, refinement_growth)
+                        mixed.reduced_time_share, scheme, 0, round_reduction)
 
 
-DEFAULT_SCHEME = MIXED_TWO_PASS
+DEFAULT_SCHEME = MIXED_REFINEMENT
 
 
 def mixed_solve(problem: LpProblem, params: PdhgParams = PdhgParams(),
                 mixed: MixedPrecisionParams = MixedPrecisionParams(), scheme: int = None,
-                cancel: Optional[C.c_int32] = None, device: int = 0, max_refinements: int = 8,
-                refinement_growth: float = 1e4, ctx: Optional[Context] = None) -> MixedPrecisionResult:
+                cancel: Optional[C.c_int32] = None, device: int = 0, round_reduction: float = 0.0,
+                ctx: Optional[Context] = None) -> MixedPrecisionResult:
     """``MixedPrecision.solve`` with both passes on the GPU."""
     scheme = DEFAULT_SCHEME if scheme is None else scheme
     ctx = ctx or context(device, 32)
@@ -386,7 +386,7 @@ def mixed_solve(problem: LpProblem, params: PdhgParams = PdhgParams(),
     x, y, rc = np.zeros(n), np.zeros(m), np.zeros(n)
     info, minfo = CInfo(), CMixedInfo()
     cp = to_c_params(params)
-    mp = to_c_mixed(mixed, scheme, max_refinements, refinement_growth)
+    mp = to_c_mixed(mixed, scheme, round_reduction)
     _check(ctx.lib.prima_mixed_solve(ctx.handle, C.byref(lpv.c), C.byref(cp), C.byref(mp),
                                      None if cancel is None else C.cast(C.byref(cancel), _IP), _dp(x), _dp(y),
                                      _dp(rc), C.byref(info), C.byref(minfo)))
@@ -431,11 +431,11 @@ class DeviceProblem:
 
     def mixed_solve(self, params: PdhgParams = PdhgParams(), mixed: MixedPrecisionParams = MixedPrecisionParams(),
                     scheme: int = None, cancel: Optional[C.c_int32] = None, want_solution: bool = True,
-                    max_refinements: int = 8, refinement_growth: float = 1e4) -> MixedPrecisionResult:
+                    round_reduction: float = 0.0) -> MixedPrecisionResult:
         scheme = DEFAULT_SCHEME if scheme is None else scheme
         x, y, rc = self._outs(want_solution)
         info, minfo = CInfo(), CMixedInfo()
-        mp = to_c_mixed(mixed, scheme, max_refinements, refinement_growth)
+        mp = to_c_mixed(mixed, scheme, round_reduction)
         _check(self.ctx.lib.prima_problem_mixed_solve(self.ctx.handle, self.handle, C.byref(to_c_params(params)),
                                                       C.byref(mp),
                                                       None if cancel is None else C.cast(C.byref(cancel), _IP),
