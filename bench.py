@@ -304,7 +304,7 @@ def main():
 # DRAM bytes (read + write) per step-size trial of pdhg_kernel<float> on this
 # workload, from an ncu capture of a bounded run of the same instance; None
 # until measured.
-TRAFFIC_BYTES_PER_TRIAL = None
+TRAFFIC_BYTES_PER_TRIAL = 151.3e6
 
 if __name__ == "__main__":
     main()
