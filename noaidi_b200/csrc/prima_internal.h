@@ -78,6 +78,8 @@ struct PreparedLp {
   double orig_spectral_bound = 0, scaled_spectral_bound = 0, rhs_norm = 0, obj_norm = 0;
   double scaled_c_norm = 0, scaled_q_norm = 0;
   std::vector<double> h_sc, h_sq, h_sl, h_su, h_cs, h_rs;  // host copies for warm starts
+  std::vector<int32_t> h_kp, h_tp;                       // row pointers of K and K'
+  int32_t hot_rows[2][2] = {{0, 0}, {0, 0}};             // [precision][K, K'] streamed tile rows
   std::unique_ptr<LpHostCopy> owned;  // the caller's problem, when held by a handle
   const prima_lp *host = nullptr;     // the caller's problem (valid while in use)
 

@@ -28,11 +28,14 @@ void DeviceBuffer::release() {
   bytes = 0;
 }
 
+// Every buffer carries 64 bytes of slack past its logical end: bulk copies
+// into shared memory move whole 16-byte granules, so a copy of a range that
+// ends mid-granule reads (and discards) up to 12 bytes beyond it.
 int32_t DeviceBuffer::reserve(size_t b) {
   if (b <= bytes && ptr) return PRIMA_OK;
   release();
   if (b == 0) b = 256;
-  cudaError_t e = cudaMalloc(&ptr, b);
+  cudaError_t e = cudaMalloc(&ptr, b + 64);
   if (e != cudaSuccess) {
     ptr = nullptr;
     set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));

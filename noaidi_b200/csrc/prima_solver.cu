@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <thread>
@@ -45,9 +47,10 @@ __device__ __forceinline__ T ldv(const T *p) {
   return __ldcg(p);
 }
 
-// Each block owns one contiguous chunk of rows (resp. columns).
+// Each block owns one contiguous chunk of rows (resp. columns); chunks start
+// at multiples of 4 so every bulk copy of a vector slice is 16-byte aligned.
 __device__ __forceinline__ void chunk(int32_t total, int nb, int rank, int32_t &lo, int32_t &hi) {
-  const int64_t per = ((int64_t)total + nb - 1) / nb;
+  const int64_t per = ((((int64_t)total + nb - 1) / nb) + 3) & ~(int64_t)3;
   int64_t a = (int64_t)rank * per, b = a + per;
   if (a > total) a = total;
   if (b > total) b = total;
@@ -110,13 +113,216 @@ __device__ __forceinline__ void csr_tiles(int32_t lo, int32_t hi, const int32_t 
 
 struct None {};
 
+// ---- TMA-prefetched tiles for the hot phases -------------------------------
+//
+// Phases A and B stream each tile's contiguous data -- its row pointers,
+// column indices and values, and up to six vector slices -- into shared
+// memory with one-dimensional bulk copies (cp.async.bulk, completion on an
+// mbarrier), through kStages buffers: tiles t+1 .. t+kStages-1 are in flight
+// while tile t computes, so only the gathers of x (an L2-resident vector) stay
+// on the critical path.  Every wait is bounded.
+
+// Per precision: rows per tile (at most), nonzeros per stage, stages.
+#ifndef PRIMA_HOT_F32_ROWS
+#define PRIMA_HOT_F32_ROWS 256
+#define PRIMA_HOT_F32_CAP 2048
+#define PRIMA_HOT_F32_STAGES 2
+#endif
+#ifndef PRIMA_HOT_F64_ROWS
+#define PRIMA_HOT_F64_ROWS 256
+#define PRIMA_HOT_F64_CAP 1536
+#define PRIMA_HOT_F64_STAGES 2
+#endif
+template <int R, int C, int S>
+struct HotShape {
+  static constexpr int kRows = R, kCap = C, kStages = S;
+};
+template <typename T>
+struct Hot;
+template <>
+struct Hot<float> : HotShape<PRIMA_HOT_F32_ROWS, PRIMA_HOT_F32_CAP, PRIMA_HOT_F32_STAGES> {};
+template <>
+struct Hot<double> : HotShape<PRIMA_HOT_F64_ROWS, PRIMA_HOT_F64_CAP, PRIMA_HOT_F64_STAGES> {};
+constexpr int kHotVec = 6;   // vector slices per tile, at most
+constexpr int kHotTiles = 128;  // tiles per boundary batch
+
+template <typename T>
+struct HotLayout {
+  static constexpr int kRows = Hot<T>::kRows;
+  static constexpr int kCapX = Hot<T>::kCap + 8;  // + the 16-byte rounding at both ends
+  static constexpr size_t rp_bytes = (((size_t)kRows + 4) * 4 + 15) / 16 * 16;
+  static constexpr size_t ci_off = rp_bytes;
+  static constexpr size_t v_off = ci_off + (size_t)kCapX * 4;
+  static constexpr size_t vec_off = (v_off + (size_t)kCapX * sizeof(T) + 15) / 16 * 16;
+  static constexpr size_t vec_stride = (size_t)kRows * sizeof(T);
+  static constexpr size_t buf_bytes = vec_off + kHotVec * vec_stride;
+  static constexpr int kStages = Hot<T>::kStages;
+  static constexpr size_t total = kStages * buf_bytes;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned bytes, uint64_t *b) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(b))
+               : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+constexpr long long kMbarSpinLimit = 1ll << 24;  // try_wait polls; each may suspend briefly
+
+// Bounded wait for a buffer's bulk copies.  False: gave up (the caller
+// raises the team's abort flag and leaves).
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity) {
+  for (long long i = 0; i < kMbarSpinLimit; i++)
+    if (mbar_try_wait(b, parity)) return true;
+  return false;
+}
+
+struct HotShared {
+  uint64_t bars[Hot<float>::kStages > Hot<double>::kStages ? Hot<float>::kStages : Hot<double>::kStages];
+  int32_t kb[kHotTiles + 1];
+  int flag;
+};
+
+// The streamed tile engine.  rp == nullptr: no SpMV, vectors only.  epi(r,
+// i, acc, slices) sees the row, its index in the tile, the row's product
+// (index-order sum from zero, as csr_tiles) and the tile's vector slices.
+template <typename T, typename Epi>
+__device__ __forceinline__ bool hot_tiles(int32_t lo, int32_t hi, int R, const int32_t *__restrict__ rp,
+                                          const int32_t *__restrict__ ci, const T *__restrict__ v, const T *xg,
+                                          const T *const *vecs, int nv, unsigned char *smem, HotShared &hs,
+                                          unsigned &par, int32_t *abort_flag, Epi &&epi) {
+  using L = HotLayout<T>;
+  constexpr int S = L::kStages;
+  const bool spmv = rp != nullptr;
+  bool ok = true;
+  for (int32_t base = lo; base < hi && ok; base += kHotTiles * R) {
+    const int32_t end = min(hi, base + kHotTiles * R);
+    const int nt = (end - base + R - 1) / R;
+    if (spmv)
+      for (int t = threadIdx.x; t <= nt; t += kThreads) hs.kb[t] = __ldg(rp + min(base + t * R, end));
+    if (threadIdx.x == 0) hs.flag = 0;
+    __syncthreads();
+    auto issue = [&](int t) {  // thread 0
+      const int b = t % S;
+      unsigned char *buf = smem + b * L::buf_bytes;
+      const int32_t r0 = base + t * R, rows = min(end, r0 + R) - r0;
+      const unsigned vb = ((unsigned)rows * (unsigned)sizeof(T) + 15u) & ~15u;
+      unsigned total = (unsigned)nv * vb, rpb = 0, cb = 0, vvb = 0;
+      int32_t ka = 0;
+      if (spmv) {
+        rpb = ((unsigned)(rows + 1) * 4u + 15u) & ~15u;
+        const int32_t k0 = hs.kb[t], k1 = hs.kb[t + 1];
+        ka = k0 & ~3;
+        const int32_t kbnd = (k1 + 3) & ~3;
+        if (kbnd - ka <= L::kCapX && kbnd > ka) {
+          cb = (unsigned)(kbnd - ka) * 4u;
+          vvb = (unsigned)(kbnd - ka) * (unsigned)sizeof(T);
+        }
+        total += rpb + cb + vvb;
+      }
+      fence_proxy_async();
+      mbar_expect_tx(&hs.bars[b], total);
+      for (int i = 0; i < nv; i++) bulk_copy(buf + L::vec_off + i * L::vec_stride, vecs[i] + r0, vb, &hs.bars[b]);
+      if (spmv) {
+        bulk_copy(buf, rp + r0, rpb, &hs.bars[b]);
+        if (cb) {
+          bulk_copy(buf + L::ci_off, ci + ka, cb, &hs.bars[b]);
+          bulk_copy(buf + L::v_off, v + ka, vvb, &hs.bars[b]);
+        }
+      }
+    };
+    if (threadIdx.x == 0)
+      for (int t = 0; t < S - 1 && t < nt; t++) issue(t);
+    for (int t = 0; t < nt; t++) {
+      if (threadIdx.x == 0 && t + S - 1 < nt) issue(t + S - 1);
+      const int b = t % S;
+      if (!mbar_wait(&hs.bars[b], (par >> b) & 1u)) {
+        atomicExch(abort_flag, 1);
+        hs.flag = 1;
+      }
+      par ^= 1u << b;
+      __syncthreads();
+      if (hs.flag) {  // leave; first let the prefetched tiles land (bounded)
+        for (int u = t + 1; u < nt && u < t + S; u++) {
+          mbar_wait(&hs.bars[u % S], (par >> (u % S)) & 1u);
+          par ^= 1u << (u % S);
+        }
+        ok = false;
+        break;
+      }
+      unsigned char *buf = smem + b * L::buf_bytes;
+      const int32_t r0 = base + t * R, rows = min(end, r0 + R) - r0;
+      const int32_t *rp_s = reinterpret_cast<const int32_t *>(buf);
+      const int32_t *ci_s = reinterpret_cast<const int32_t *>(buf + L::ci_off);
+      T *v_s = reinterpret_cast<T *>(buf + L::v_off);
+      const T *slices = reinterpret_cast<const T *>(buf + L::vec_off);
+      int32_t ka = 0;
+      bool staged = false;
+      if (spmv) {
+        const int32_t k0 = hs.kb[t], k1 = hs.kb[t + 1];
+        ka = k0 & ~3;
+        const int32_t kbnd = (k1 + 3) & ~3;
+        staged = kbnd - ka <= L::kCapX;
+        if (staged) {
+#pragma unroll 4
+          for (int32_t k = k0 + threadIdx.x; k < k1; k += kThreads) v_s[k - ka] = v_s[k - ka] * ldv(xg + ci_s[k - ka]);
+        }
+        __syncthreads();
+      }
+      // row r goes to thread (r - lo) mod kThreads whatever R is, so each
+      // thread's running totals (and the block reductions) keep one order
+      const int rot = (t * R) & (kThreads - 1);
+      for (int i = (threadIdx.x - rot) & (kThreads - 1); i < rows; i += kThreads) {
+        T acc = T(0);
+        if (spmv) {
+          const int32_t a0 = rp_s[i], a1 = rp_s[i + 1];
+          if (staged) {
+            for (int32_t k = a0; k < a1; k++) acc = acc + v_s[k - ka];
+          } else {
+            for (int32_t k = a0; k < a1; k++) acc = acc + (__ldg(v + k) * ldv(xg + __ldg(ci + k)));
+          }
+        }
+        epi(r0 + i, i, acc, slices);
+      }
+      __syncthreads();
+    }
+  }
+  return ok;
+}
+
+// One shared staging area for every block reduction (a single allocation
+// per block, whatever the number of template instances).
+__device__ __forceinline__ double (&reduction_scratch())[kMaxQ][kWarps] {
+  __shared__ double sh[kMaxQ][kWarps];
+  return sh;
+}
+
 // Block-wide totals of Q per-thread values in a fixed order.  The block's
 // totals go to shared s_part[base..base+Q) and, in a multi-block team, to the
 // global partials[(base + q) * stride + rank].
 template <int Q>
 __device__ __forceinline__ void block_partials(const double (&v)[Q], double *partials, int stride, int rank, int nb,
                                                int base, double *s_part) {
-  __shared__ double sh[kMaxQ][kWarps];
+  double(&sh)[kMaxQ][kWarps] = reduction_scratch();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < Q; q++) {
@@ -146,7 +352,7 @@ __device__ __forceinline__ void reduce_partials(const double *partials, int stri
     __syncthreads();
     return;
   }
-  __shared__ double sh[kMaxQ][kWarps];
+  double(&sh)[kMaxQ][kWarps] = reduction_scratch();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double v[Q];
 #pragma unroll
@@ -452,46 +658,56 @@ __device__ void phase_init(const Args<T> &a, const Control &s, const Team &tm, T
 }
 
 // Primal half of a trial (primalStep + extrapolation), fused with the
-// pending commit's K'y and running sums.
+// pending commit's K'y and running sums; operands streamed by TMA.
 template <typename T>
-__device__ void phase_a(const Args<T> &a, const Control &s, const Team &tm, T *s_prod) {
+__device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsigned char *smem, HotShared &hs,
+                        unsigned &par) {
+  using L = HotLayout<T>;
   double v[1] = {0.0};
   int32_t lo, hi;
   chunk(a.n, tm.nb, tm.rank, lo, hi);
   const T tau = (T)s.tau, w = (T)s.pend_w;
   const T *x = a.x[s.xc];
   T *xn_out = a.x[s.xc ^ 1];
-  auto step = [&](int32_t j, T xj, T kt) {
+  auto step = [&](int32_t j, T xj, T kt, T cj, T lj, T uj) {
     // ScalaKernels.primalStep (:78-98): two-comparison clamp
-    const T st = xj - (tau * (ldv(a.c + j) - kt));
-    const T lj = ldv(a.l + j), uj = ldv(a.u + j);
+    const T st = xj - (tau * (cj - kt));
     const T xn = st < lj ? lj : (st > uj ? uj : st);
     xn_out[j] = xn;
     a.xbar[j] = (T(2) * xn) + (T(-1) * xj);
     const T d = (T(1) * xn) + (T(-1) * xj);
     v[0] += (double)d * (double)d;
   };
+  bool ok;
   if (s.pend) {
-    struct Ops {
-      T x, sx, skty;
-    };
-    csr_tiles<T>(lo, hi, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], s_prod,
-                 [&](int32_t j) { return Ops{ldv(x + j), ldv(a.sx + j), ldv(a.skty + j)}; },
-                 [&](int32_t j, T kt, const Ops &o) {
-      a.kty[j] = kt;
-      a.sx[j] = (w * o.x) + (T(1) * o.sx);
-      a.skty[j] = (w * kt) + (T(1) * o.skty);
-      step(j, o.x, kt);
-    });
+    const T *vecs[6] = {x, a.sx, a.skty, a.c, a.l, a.u};
+    ok = hot_tiles<T>(lo, hi, a.rows_t, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], vecs, 6, smem, hs, par, &a.sync->abort,
+                      [&](int32_t j, int i, T kt, const T *sl) {
+                        constexpr int S = L::kRows;
+                        const T xj = sl[i], sx = sl[S + i], skt = sl[2 * S + i];
+                        a.kty[j] = kt;
+                        a.sx[j] = (w * xj) + (T(1) * sx);
+                        a.skty[j] = (w * kt) + (T(1) * skt);
+                        step(j, xj, kt, sl[3 * S + i], sl[4 * S + i], sl[5 * S + i]);
+                      });
   } else {
-    for (int32_t j = lo + threadIdx.x; j < hi; j += kThreads) step(j, ldv(x + j), ldv(a.kty + j));
+    const T *vecs[5] = {x, a.kty, a.c, a.l, a.u};
+    ok = hot_tiles<T>(lo, hi, L::kRows, nullptr, nullptr, nullptr, nullptr, vecs, 5, smem, hs, par, &a.sync->abort,
+                      [&](int32_t j, int i, T, const T *sl) {
+                        constexpr int S = L::kRows;
+                        step(j, sl[i], sl[S + i], sl[2 * S + i], sl[3 * S + i], sl[4 * S + i]);
+                      });
   }
   block_partials<1>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DX, tm.s_part);
+  return ok;
 }
 
-// Dual half of a trial: K xbar, dualStep, the speculative kx commit value.
+// Dual half of a trial: K xbar, dualStep, the speculative kx commit value;
+// operands streamed by TMA.
 template <typename T>
-__device__ void phase_b(const Args<T> &a, const Control &s, const Team &tm, T *s_prod) {
+__device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsigned char *smem, HotShared &hs,
+                        unsigned &par) {
+  using L = HotLayout<T>;
   double v[2] = {0.0, 0.0};
   int32_t lo, hi;
   chunk(a.m, tm.nb, tm.rank, lo, hi);
@@ -501,29 +717,28 @@ __device__ void phase_b(const Args<T> &a, const Control &s, const Team &tm, T *s
   T *y_out = a.y[s.yc ^ 1];
   T *kx_out = a.kx[s.kxc ^ 1];
   const bool pend = s.pend != 0;
-  struct Ops {
-    T y, kx, q, sy, skx;
-  };
-  csr_tiles<T>(lo, hi, a.kp, a.kci, a.kv, (const T *)a.xbar, s_prod,
-               [&](int32_t r) {
-                 Ops o{ldv(y + r), ldv(kx + r), ldv(a.q + r), T(0), T(0)};
-                 if (pend) {
-                   o.sy = ldv(a.sy + r);
-                   o.skx = ldv(a.skx + r);
-                 }
-                 return o;
-               },
-               [&](int32_t r, T kb, const Ops &o) {
-    const T yr = o.y, kxr = o.kx;
+  const T *vecs[6] = {y, kx, a.q, a.sy, a.skx, a.ylo};
+  int nv = 3;
+  if (pend) nv = 5;
+  const int iylo = nv;
+  if (a.ylo) {
+    vecs[nv] = a.ylo;
+    nv++;
+  }
+  const bool has_lo = a.ylo != nullptr;
+  const bool ok = hot_tiles<T>(lo, hi, a.rows_k, a.kp, a.kci, a.kv, (const T *)a.xbar, vecs, nv, smem, hs, par, &a.sync->abort,
+                               [&](int32_t r, int i, T kb, const T *sl) {
+    constexpr int S = L::kRows;
+    const T yr = sl[i], kxr = sl[S + i], qr = sl[2 * S + i];
     if (pend) {
-      a.sy[r] = (w * yr) + (T(1) * o.sy);
-      a.skx[r] = (w * kxr) + (T(1) * o.skx);
+      a.sy[r] = (w * yr) + (T(1) * sl[3 * S + i]);
+      a.skx[r] = (w * kxr) + (T(1) * sl[4 * S + i]);
     }
-    // ScalaKernels.dualStep (:100-118)
-    T yn = yr + (sigma * (o.q - kb));
-    if (r >= a.neq) {  // the cone y >= 0, or y^ >= -ya around an anchor
-      const T lo = a.ylo ? ldv(a.ylo + r) : T(0);
-      yn = yn > lo ? yn : lo;
+    // ScalaKernels.dualStep (:100-118); around an anchor the cone is y >= -ya
+    T yn = yr + (sigma * (qr - kb));
+    if (r >= a.neq) {
+      const T lb = has_lo ? sl[iylo * S + i] : T(0);
+      yn = yn > lb ? yn : lb;
     }
     y_out[r] = yn;
     kx_out[r] = (T(0.5) * kb) + (T(0.5) * kxr);
@@ -533,6 +748,7 @@ __device__ void phase_b(const Args<T> &a, const Control &s, const Team &tm, T *s
     v[1] += (double)dy * (double)kdx;
   });
   block_partials<2>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DY, tm.s_part);
+  return ok;
 }
 
 // Flush the pending commit, optionally refresh kx = K x, evaluate the
@@ -728,6 +944,14 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
       break;
     }
     case PH_B: {  // Solve.step's trial decision, Pdhg.scala:336-380
+      // the step rule's two powers depend only on the iteration count: two
+      // other warps evaluate them while the partials are being reduced
+      __shared__ double s_pow[2];
+      {
+        const double t = (double)(c.iteration - c.period_base + 1);
+        if (threadIdx.x == 32) s_pow[0] = pow(t, -0.3);
+        if (threadIdx.x == 64) s_pow[1] = pow(t, -0.6);
+      }
       reduce_partials<3>(a.partials, a.max_blocks, tm.nb, tm.s_part, red);
       if (threadIdx.x == 0) {
         c.trials += 1;
@@ -744,9 +968,8 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
         } else {
           const double interaction = fabs(red[Q_INTER]);
           const double limit = interaction > 0.0 ? movement / interaction : CUDART_INF;
-          const double t = (double)(c.iteration - c.period_base + 1);
-          const double by_rule = (1.0 - pow(t, -0.3)) * limit;
-          const double by_cap = (1.0 + pow(t, -0.6)) * c.step;
+          const double by_rule = (1.0 - s_pow[0]) * limit;
+          const double by_cap = (1.0 + s_pow[1]) * c.step;
           const double proposed = dmin(by_rule, by_cap);
           const bool accept = c.step <= limit || c.trials >= 60;
           if (accept) {
@@ -916,10 +1139,25 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
   __shared__ double s_red[kMaxQ];
   if (tm.nb == 1) {
     __syncthreads();
+    if (*((volatile int32_t *)&a.sync->abort)) return false;
+    uint64_t t0 = 0;
+    if (threadIdx.x == 0) {
+      t0 = global_timer_ns();
+      if (a.prof->t_release) {
+        a.prof->phase_ns[phase & 7] += t0 - a.prof->t_release;
+        a.prof->phase_count[phase & 7] += 1;
+      }
+    }
     if (phase == PH_A) {
       if (threadIdx.x == 0) snap.phase = PH_B;
     } else {
       decide<T>(a, snap, phase, tm, s_red);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint64_t t1 = global_timer_ns();
+      a.prof->decide_ns += t1 - t0;
+      a.prof->t_release = t1;
     }
     __syncthreads();
     return true;
@@ -933,6 +1171,15 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
   }
   __syncthreads();
   if (s_last) {
+    __shared__ uint64_t s_t0;
+    if (threadIdx.x == 0) {
+      s_t0 = global_timer_ns();
+      const uint64_t tr = ldv(&a.prof->t_release);
+      if (tr) {
+        a.prof->phase_ns[phase & 7] += s_t0 - tr;
+        a.prof->phase_count[phase & 7] += 1;
+      }
+    }
     if (phase == PH_A) {
       if (threadIdx.x == 0) snap.phase = PH_B;
     } else {
@@ -940,6 +1187,11 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     }
     __syncthreads();
     if (phase != PH_A) publish_control(a, snap);
+    if (threadIdx.x == 0) {
+      const uint64_t t1 = global_timer_ns();
+      a.prof->decide_ns += t1 - s_t0;
+      a.prof->t_release = t1;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
       if (*((volatile int32_t *)&a.sync->abort)) s_ok = 0;
@@ -972,23 +1224,31 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, kMinBlocksPerSm) pdhg_kernel(Args<T> a) {
   __shared__ Control snap;
   __shared__ double s_part[kMaxQ];
-  extern __shared__ __align__(16) unsigned char s_dyn[];
+  __shared__ HotShared hs;
+  extern __shared__ __align__(128) unsigned char s_dyn[];
   T *s_prod = reinterpret_cast<T *>(s_dyn);
   const Team tm{(int)gridDim.x, (int)blockIdx.x, s_part};
-  load_control(a, snap);
+  unsigned par = 0;  // mbarrier phase parity of the two tile buffers
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < HotLayout<T>::kStages; i++) mbar_init(&hs.bars[i], 1);
+    fence_mbar_init();
+  }
+  load_control(a, snap);  // (syncs the block)
   for (;;) {
     const int ph = snap.phase;
     if (ph == PH_DONE) break;
+    bool ok = true;
     switch (ph) {
       case PH_INIT: phase_init(a, snap, tm, s_prod); break;
-      case PH_A: phase_a(a, snap, tm, s_prod); break;
-      case PH_B: phase_b(a, snap, tm, s_prod); break;
+      case PH_A: ok = phase_a(a, snap, tm, s_dyn, hs, par); break;
+      case PH_B: ok = phase_b(a, snap, tm, s_dyn, hs, par); break;
       case PH_F: phase_f(a, snap, tm, s_prod); break;
       case PH_R: phase_r(a, snap, tm); break;
       case PH_W: phase_w(a, snap, tm); break;
       case PH_R2: phase_r2(a, snap, tm, s_prod); break;
       default: break;
     }
+    (void)ok;  // a failed tile wait has raised the team's abort flag; the barrier sees it
     if (!barrier_decide(a, snap, ph, tm)) break;
   }
   if (tm.nb == 1) publish_control(a, snap);  // the host reads the final record
@@ -1015,14 +1275,15 @@ struct Layout {
   template <typename U>
   size_t take(int64_t count) {
     const size_t at = off;
-    off += ((size_t)std::max<int64_t>(count, 1) * sizeof(U) + 255) & ~(size_t)255;
+    // 64 bytes of slack per buffer: bulk copies move whole 16-byte granules
+    off += ((size_t)std::max<int64_t>(count, 1) * sizeof(U) + 64 + 255) & ~(size_t)255;
     return at;
   }
 };
 
 template <typename T>
 struct StateLayout {
-  size_t x[2], y[2], kx[2], xbar, kty, sx, sy, skx, skty, xr, yr, xo, yo, rco, part, ctl, sync, bytes;
+  size_t x[2], y[2], kx[2], xbar, kty, sx, sy, skx, skty, xr, yr, xo, yo, rco, part, ctl, sync, prof, bytes;
   size_t xa = 0, ya = 0, kxa = 0, ktya = 0, cw = 0, lw = 0, uw = 0, qw = 0, ylo = 0;
   StateLayout(int32_t n, int32_t m, int blocks, bool anchored) {
     Layout L;
@@ -1056,13 +1317,14 @@ struct StateLayout {
     part = L.take<double>((int64_t)dev::kMaxQ * blocks);
     ctl = L.take<dev::Control>(1);
     sync = L.take<dev::Sync>(1);
+    prof = L.take<dev::Prof>(1);
     bytes = L.off;
   }
 };
 
 template <typename T>
 constexpr size_t dyn_smem() {
-  return (size_t)dev::kTileCap * sizeof(T);
+  return std::max((size_t)dev::kTileCap * sizeof(T), dev::HotLayout<T>::total);
 }
 
 template <typename T>
@@ -1086,6 +1348,25 @@ inline int team_blocks(int64_t n, int64_t m, int max_blocks) {
   const int64_t work = std::max<int64_t>(std::max(n, m), 1);
   if (work <= 4096) return 1;
   return (int)std::min<int64_t>(max_blocks, (work + dev::kTileRows - 1) / dev::kTileRows);
+}
+
+// Rows per streamed tile: the largest power of two (<= 256) for which at most
+// 1/32 of the windows of that many rows, starting at a multiple of 4, hold
+// more nonzeros (rounded out to 16-byte granules) than one stage.  Fewer,
+// larger tiles beat fully staged small ones: a tile that does not fit reads
+// its indices and values from global memory instead.
+template <typename T>
+int32_t hot_rows(const std::vector<int32_t> &rp) {
+  const int64_t rows = (int64_t)rp.size() - 1, capx = dev::HotLayout<T>::kCapX;
+  for (int32_t R = dev::HotLayout<T>::kRows; R >= 4; R /= 2) {
+    int64_t over = 0, windows = 0;
+    for (int64_t r0 = 0; r0 < rows; r0 += 4, windows++) {
+      const int64_t r1 = std::min<int64_t>(rows, r0 + R);
+      if (((rp[r1] + 3) & ~3) - (rp[r0] & ~3) > capx) over++;
+    }
+    if (over * 32 <= windows) return R;
+  }
+  return 4;
 }
 
 template <typename T>
@@ -1218,6 +1499,13 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   a.max_blocks = blocks;
   a.ctl = (dev::Control *)(base + S.ctl);
   a.sync = (dev::Sync *)(base + S.sync);
+  a.prof = (dev::Prof *)(base + S.prof);
+  if (!L.hot_rows[w][0]) {
+    L.hot_rows[w][0] = hot_rows<T>(L.h_kp);
+    L.hot_rows[w][1] = hot_rows<T>(L.h_tp);
+  }
+  a.rows_k = L.hot_rows[w][0];
+  a.rows_t = L.hot_rows[w][1];
   if (anchored) {
     a.anchored = 1;
     a.xa = (double *)(base + S.xa);
@@ -1255,6 +1543,7 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   std::memset(&sync, 0, sizeof(sync));
   PRIMA_CUDA_TRY(cudaMemcpyAsync(a.ctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
   PRIMA_CUDA_TRY(cudaMemcpyAsync(a.sync, &sync, sizeof(sync), cudaMemcpyHostToDevice, s));
+  PRIMA_CUDA_TRY(cudaMemsetAsync(a.prof, 0, sizeof(dev::Prof), s));
 
   dev::Params &P = a.P;
   P.eps_abs = p->eps_abs;
@@ -1331,6 +1620,19 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   info->trials = ctl.total_trials;
   info->solve_ms = (int64_t)ms_since(t_start);
   if (req.rounds) *req.rounds = ctl.rounds;
+  if (std::getenv("PRIMA_PHASE_TIMES")) {
+    dev::Prof prof;
+    PRIMA_CUDA_TRY(cudaMemcpy(&prof, a.prof, sizeof(prof), cudaMemcpyDeviceToHost));
+    static const char *names[8] = {"init", "A", "B", "F", "R", "W", "-", "R2"};
+    std::fprintf(stderr, "[prima] blocks=%d rows=%d/%d trials=%lld decide %.2f us/barrier:", blocks, a.rows_k,
+                 a.rows_t, (long long)ctl.total_trials,
+                 1e-3 * (double)prof.decide_ns / std::max<int64_t>(1, 2 * ctl.total_trials));
+    for (int k = 0; k < 8; k++)
+      if (prof.phase_count[k])
+        std::fprintf(stderr, " %s %.2f us x%lld", names[k], 1e-3 * (double)prof.phase_ns[k] / (double)prof.phase_count[k],
+                     (long long)prof.phase_count[k]);
+    std::fprintf(stderr, "\n");
+  }
   if (ctl.error) {
     set_error("a bounded device-side wait gave up; the solve was abandoned");
     return PRIMA_ERR_TIMEOUT;

@@ -40,7 +40,10 @@ namespace dev {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMinBlocksPerSm = 4;  // register cap 64: enough warps in flight for the gathers
+#ifndef PRIMA_MIN_BLOCKS_PER_SM
+#define PRIMA_MIN_BLOCKS_PER_SM 4
+#endif
+constexpr int kMinBlocksPerSm = PRIMA_MIN_BLOCKS_PER_SM;  // register cap 64: enough warps in flight for the gathers
 constexpr int kTileRows = 512;      // rows of one CSR-stream tile (2 per thread)
 constexpr int kRowsPerThread = kTileRows / kThreads;
 constexpr int kTileCap = 4096;      // staged products per tile (dynamic shared memory)
@@ -114,6 +117,16 @@ struct Sync {
   int32_t pad;
 };
 
+// Phase timing, kept by whichever block decides (one at a time): time from a
+// barrier's release to the last block's arrival at the next one, per phase
+// kind, and the deciding block's own time.
+struct Prof {
+  uint64_t t_release;
+  uint64_t decide_ns;
+  uint64_t phase_ns[8];
+  int64_t phase_count[8];
+};
+
 template <typename T>
 struct Args {
   int32_t n, m, neq, pad;
@@ -133,6 +146,8 @@ struct Args {
   double *xo, *yo, *rco;
   double *partials;  // [kMaxQ][max_blocks]
   int32_t max_blocks, anchored;
+  int32_t rows_k, rows_t;  // rows per streamed tile of K and of K' (their nonzeros fit the stage)
+  Prof *prof;
   // Anchored (refinement) mode: the iterate is a correction (x^, y^) to an
   // FP64 anchor (xa, ya) whose exact products kxa = K xa, ktya = K'ya are
   // kept; the working data c, q, l, u, ylo are the residual problem
