@@ -95,6 +95,20 @@ int32_t prima_scale(prima_handle ctx, double alpha, prima_handle x, prima_handle
 int32_t prima_copy(prima_handle ctx, prima_handle src, prima_handle dst);
 int32_t prima_dot(prima_handle ctx, prima_handle x, prima_handle y, double *out);
 int32_t prima_squared_norm(prima_handle ctx, prima_handle x, double *out);
+/* No counterpart in the reference.  prima_dot without a context and without
+ * any allocation, for callers that own their device memory and must not see
+ * a library cudaMalloc/cudaFree (cudaFree synchronises the device): *out :=
+ * sum x[i]*y[i] accumulated in double, x and y arrays of n floats
+ * (element_bits 32) or doubles (64), x, y and out device pointers on the
+ * calling thread's current device, enqueued on `stream` (a cudaStream_t;
+ * NULL is the default stream) and not waited for.  n at most 16,777,216;
+ * larger n is rejected with PRIMA_ERR_INVALID_ARGUMENT.  The block partials
+ * live in a fixed 16 KiB device array that every GPU loading the library
+ * holds until exit; the first call on each device looks up its address and
+ * should come before any stream capture.  Calls that overlap on the GPU race
+ * on that array. */
+int32_t prima_dot_no_alloc(const void *x, const void *y, int64_t n, int32_t element_bits, double *out,
+                           void *stream);
 /* out := clamp(x - tau*(cost - kty), lower, upper), two-comparison clamp */
 int32_t prima_primal_step(prima_handle ctx, prima_handle x, prima_handle kty, prima_handle cost,
                           prima_handle lower, prima_handle upper, double tau, prima_handle out);

@@ -107,6 +107,7 @@ SIGNATURES = {
     "prima_copy": (C.c_int32, [_H, _H, _H]),
     "prima_dot": (C.c_int32, [_H, _H, _H, _DP]),
     "prima_squared_norm": (C.c_int32, [_H, _H, _DP]),
+    "prima_dot_no_alloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     "prima_primal_step": (C.c_int32, [_H, _H, _H, _H, _H, _H, C.c_double, _H]),
     "prima_dual_step": (C.c_int32, [_H, _H, _H, _H, C.c_double, C.c_int32, _H]),
     "prima_params_default": (None, [C.POINTER(CParams)]),
