@@ -166,6 +166,21 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_profile_case(args) -> None:
+    """A bounded run for profilers: the workload (optionally fewer snapshots)
+    resident on the device, one plain PDHG solve capped at
+    --profile-iterations iterations in the chosen precision."""
+    from noaidi_b200.prima import PdhgParams, cuda, generators as G
+    problem = G.dc_lopf(seed=0, **dict(WORKLOAD, snapshots=args.profile_snapshots))
+    params = PdhgParams(eps_abs=EPS, eps_rel=EPS, max_iterations=args.profile_iterations)
+    resident = cuda.DeviceProblem(problem, params, precision=args.profile_precision)
+    s = resident.solve(params, want_solution=False)
+    print(json.dumps({"profile_case": True, "precision": args.profile_precision, "n": problem.num_variables,
+                      "m": problem.num_constraints, "nnz": problem.constraint_matrix.nnz,
+                      "iterations": s.iterations, "trials": s.trials,
+                      "us_per_trial": 1e3 * s.device_ms / max(1, s.trials)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -179,9 +194,15 @@ def main():
     ap.add_argument("--full-fp64", action="store_true", help="solve FP64 to tolerance instead of sampling")
     ap.add_argument("--cpu-sample-iterations", type=int, default=128)
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--profile-iterations", type=int, default=0,
+                    help="only run this many PDHG iterations of the workload (a bounded case for ncu) and exit")
+    ap.add_argument("--profile-precision", type=int, default=32, choices=[32, 64])
+    ap.add_argument("--profile-snapshots", type=int, default=WORKLOAD["snapshots"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_iterations:
+        return run_profile_case(args)
 
     import torch
     rank = int(os.environ.get("RANK", "0"))

@@ -79,7 +79,8 @@ struct PreparedLp {
   double scaled_c_norm = 0, scaled_q_norm = 0;
   std::vector<double> h_sc, h_sq, h_sl, h_su, h_cs, h_rs;  // host copies for warm starts
   std::vector<int32_t> h_kp, h_tp;                       // row pointers of K and K'
-  int32_t hot_rows[2][2] = {{0, 0}, {0, 0}};             // [precision][K, K'] streamed tile rows
+  DeviceBuffer b_tiles[2][2];                            // [precision][K, K'] warp-tile tables (int2)
+  int32_t ntiles[2][2] = {{0, 0}, {0, 0}};
   std::unique_ptr<LpHostCopy> owned;  // the caller's problem, when held by a handle
   const prima_lp *host = nullptr;     // the caller's problem (valid while in use)
 

@@ -277,7 +277,7 @@ int32_t PreparedLp::prepare(const prima_lp *lp, const prima_params *p, cudaStrea
   h_kp.assign(lp->row_ptr, lp->row_ptr + m + 1);
   h_tp.resize((size_t)n + 1);
   PRIMA_CUDA_TRY(cudaMemcpyAsync(h_tp.data(), b_tp.ptr, ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost, s));
-  hot_rows[0][0] = hot_rows[0][1] = hot_rows[1][0] = hot_rows[1][1] = 0;
+  ntiles[0][0] = ntiles[0][1] = ntiles[1][0] = ntiles[1][1] = 0;
   PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
   scaled_c_norm = norm2(h_sc.data(), n);
   scaled_q_norm = norm2(h_sq.data(), m);

@@ -113,51 +113,55 @@ __device__ __forceinline__ void csr_tiles(int32_t lo, int32_t hi, const int32_t 
 
 struct None {};
 
-// ---- TMA-prefetched tiles for the hot phases -------------------------------
+// ---- TMA-prefetched warp tiles for the hot phases ------------------------
 //
-// Phases A and B stream each tile's contiguous data -- its row pointers,
-// column indices and values, and up to six vector slices -- into shared
-// memory with one-dimensional bulk copies (cp.async.bulk, completion on an
-// mbarrier), through kStages buffers: tiles t+1 .. t+kStages-1 are in flight
-// while tile t computes, so only the gathers of x (an L2-resident vector) stay
-// on the critical path.  Every wait is bounded.
+// Phases A and B cut the rows of K' (A) and K (B) into warp tiles: at most
+// 32 rows, starting at a multiple of 4, whose nonzeros (rounded out to
+// 16-byte granules) fit one stage -- a table built once per matrix on the
+// host.  Each warp runs its own kStages-deep pipeline: its lane 0 streams a
+// tile's row pointers, column indices, values and up to six vector slices
+// into the warp's shared-memory stage with one-dimensional bulk copies
+// (cp.async.bulk, completion on the stage's mbarrier) while the warp works on
+// an earlier tile.  Warps never wait for one another inside a phase, so the
+// latency of one warp's gathers hides behind the other warps' streams.  Every
+// wait is bounded.
 
-// Per precision: rows per tile (at most), nonzeros per stage, stages.
-#ifndef PRIMA_HOT_F32_ROWS
-#define PRIMA_HOT_F32_ROWS 256
-#define PRIMA_HOT_F32_CAP 2048
-#define PRIMA_HOT_F32_STAGES 2
+#ifndef PRIMA_WARP_F32_CAP
+#define PRIMA_WARP_F32_CAP 192
+#define PRIMA_WARP_F32_STAGES 2
 #endif
-#ifndef PRIMA_HOT_F64_ROWS
-#define PRIMA_HOT_F64_ROWS 256
-#define PRIMA_HOT_F64_CAP 1536
-#define PRIMA_HOT_F64_STAGES 2
+#ifndef PRIMA_WARP_F64_CAP
+#define PRIMA_WARP_F64_CAP 160
+#define PRIMA_WARP_F64_STAGES 2
 #endif
-template <int R, int C, int S>
-struct HotShape {
-  static constexpr int kRows = R, kCap = C, kStages = S;
+template <int C, int S>
+struct WarpShape {
+  static_assert(C % 32 == 0, "stage capacity in whole warps");
+  static constexpr int kCap = C, kStages = S;
 };
 template <typename T>
-struct Hot;
+struct Warp;
 template <>
-struct Hot<float> : HotShape<PRIMA_HOT_F32_ROWS, PRIMA_HOT_F32_CAP, PRIMA_HOT_F32_STAGES> {};
+struct Warp<float> : WarpShape<PRIMA_WARP_F32_CAP, PRIMA_WARP_F32_STAGES> {};
 template <>
-struct Hot<double> : HotShape<PRIMA_HOT_F64_ROWS, PRIMA_HOT_F64_CAP, PRIMA_HOT_F64_STAGES> {};
-constexpr int kHotVec = 6;   // vector slices per tile, at most
-constexpr int kHotTiles = 128;  // tiles per boundary batch
+struct Warp<double> : WarpShape<PRIMA_WARP_F64_CAP, PRIMA_WARP_F64_STAGES> {};
+constexpr int kWarpRows = 32;     // rows per warp tile, at most (one per lane)
+constexpr int kWarpVec = 6;       // vector slices per tile, at most
+constexpr int kTileBatch = 256;   // tile-table entries a block stages at once
+constexpr int kMaxStages = Warp<float>::kStages > Warp<double>::kStages ? Warp<float>::kStages : Warp<double>::kStages;
 
 template <typename T>
-struct HotLayout {
-  static constexpr int kRows = Hot<T>::kRows;
-  static constexpr int kCapX = Hot<T>::kCap + 8;  // + the 16-byte rounding at both ends
-  static constexpr size_t rp_bytes = (((size_t)kRows + 4) * 4 + 15) / 16 * 16;
+struct WarpLayout {
+  static constexpr int kCap = Warp<T>::kCap;  // staged nonzeros (16-byte rounded span)
+  static constexpr int kStages = Warp<T>::kStages;
+  static constexpr size_t rp_bytes = ((size_t)(kWarpRows + 1) * 4 + 15) / 16 * 16;
   static constexpr size_t ci_off = rp_bytes;
-  static constexpr size_t v_off = ci_off + (size_t)kCapX * 4;
-  static constexpr size_t vec_off = (v_off + (size_t)kCapX * sizeof(T) + 15) / 16 * 16;
-  static constexpr size_t vec_stride = (size_t)kRows * sizeof(T);
-  static constexpr size_t buf_bytes = vec_off + kHotVec * vec_stride;
-  static constexpr int kStages = Hot<T>::kStages;
-  static constexpr size_t total = kStages * buf_bytes;
+  static constexpr size_t v_off = ci_off + (size_t)kCap * 4;
+  static constexpr size_t vec_off = (v_off + (size_t)kCap * sizeof(T) + 15) / 16 * 16;
+  static constexpr size_t vec_stride = (size_t)kWarpRows * sizeof(T);
+  static constexpr size_t stage_bytes = (vec_off + kWarpVec * vec_stride + 15) / 16 * 16;
+  static constexpr size_t warp_bytes = kStages * stage_bytes;
+  static constexpr size_t total = kWarps * warp_bytes;
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -197,116 +201,133 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity) {
 }
 
 struct HotShared {
-  uint64_t bars[Hot<float>::kStages > Hot<double>::kStages ? Hot<float>::kStages : Hot<double>::kStages];
-  int32_t kb[kHotTiles + 1];
+  uint64_t bars[kWarps * kMaxStages];  // one mbarrier per warp stage
+  int2 tiles[kTileBatch + 1];          // (first row, first nonzero) of each tile
   int flag;
 };
 
-// The streamed tile engine.  rp == nullptr: no SpMV, vectors only.  epi(r,
-// i, acc, slices) sees the row, its index in the tile, the row's product
-// (index-order sum from zero, as csr_tiles) and the tile's vector slices.
+// The warp-tile engine over tiles [tlo, thi) of a table.  rp == nullptr: no
+// SpMV, vectors only.  epi(r, i, acc, slices) runs on lane i for row r of
+// the tile: acc is the row's product (an index-order sum from zero, as
+// csr_tiles), slices the tile's vector slices (stride kWarpRows).  Returns
+// false, uniformly over the block, when the team's abort flag is up.
 template <typename T, typename Epi>
-__device__ __forceinline__ bool hot_tiles(int32_t lo, int32_t hi, int R, const int32_t *__restrict__ rp,
-                                          const int32_t *__restrict__ ci, const T *__restrict__ v, const T *xg,
-                                          const T *const *vecs, int nv, unsigned char *smem, HotShared &hs,
-                                          unsigned &par, int32_t *abort_flag, Epi &&epi) {
-  using L = HotLayout<T>;
+__device__ __forceinline__ bool hot_tiles(int32_t tlo, int32_t thi, const int2 *__restrict__ table,
+                                          const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                                          const T *__restrict__ v, const T *xg, const T *const *vecs, int nv,
+                                          unsigned char *smem, HotShared &hs, unsigned &par, int32_t *abort_flag,
+                                          Epi &&epi) {
+  using L = WarpLayout<T>;
   constexpr int S = L::kStages;
+  constexpr int U = L::kCap / 32;  // gathers per lane per tile, at most
   const bool spmv = rp != nullptr;
-  bool ok = true;
-  for (int32_t base = lo; base < hi && ok; base += kHotTiles * R) {
-    const int32_t end = min(hi, base + kHotTiles * R);
-    const int nt = (end - base + R - 1) / R;
-    if (spmv)
-      for (int t = threadIdx.x; t <= nt; t += kThreads) hs.kb[t] = __ldg(rp + min(base + t * R, end));
-    if (threadIdx.x == 0) hs.flag = 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char *wbuf = smem + (size_t)warp * L::warp_bytes;
+  uint64_t *bars = hs.bars + warp * kMaxStages;
+  for (int32_t base = tlo; base < thi; base += kTileBatch) {
+    const int nt = min(kTileBatch, thi - base);
+    for (int t = threadIdx.x; t <= nt; t += kThreads) hs.tiles[t] = __ldg(table + base + t);
     __syncthreads();
-    auto issue = [&](int t) {  // thread 0
-      const int b = t % S;
-      unsigned char *buf = smem + b * L::buf_bytes;
-      const int32_t r0 = base + t * R, rows = min(end, r0 + R) - r0;
+    const int nj = nt > warp ? (nt - warp + kWarps - 1) / kWarps : 0;  // this warp's tiles: warp + j*kWarps
+    auto issue = [&](int j) {  // lane 0
+      const int t = warp + j * kWarps, b = j % S;
+      unsigned char *buf = wbuf + b * L::stage_bytes;
+      const int2 e0 = hs.tiles[t], e1 = hs.tiles[t + 1];
+      const int32_t r0 = e0.x, rows = e1.x - e0.x;
       const unsigned vb = ((unsigned)rows * (unsigned)sizeof(T) + 15u) & ~15u;
       unsigned total = (unsigned)nv * vb, rpb = 0, cb = 0, vvb = 0;
       int32_t ka = 0;
       if (spmv) {
         rpb = ((unsigned)(rows + 1) * 4u + 15u) & ~15u;
-        const int32_t k0 = hs.kb[t], k1 = hs.kb[t + 1];
-        ka = k0 & ~3;
-        const int32_t kbnd = (k1 + 3) & ~3;
-        if (kbnd - ka <= L::kCapX && kbnd > ka) {
+        ka = e0.y & ~3;
+        const int32_t kbnd = (e1.y + 3) & ~3;
+        if (kbnd - ka <= L::kCap && kbnd > ka) {
           cb = (unsigned)(kbnd - ka) * 4u;
           vvb = (unsigned)(kbnd - ka) * (unsigned)sizeof(T);
         }
         total += rpb + cb + vvb;
       }
       fence_proxy_async();
-      mbar_expect_tx(&hs.bars[b], total);
-      for (int i = 0; i < nv; i++) bulk_copy(buf + L::vec_off + i * L::vec_stride, vecs[i] + r0, vb, &hs.bars[b]);
+      mbar_expect_tx(&bars[b], total);
+      for (int i = 0; i < nv; i++) bulk_copy(buf + L::vec_off + i * L::vec_stride, vecs[i] + r0, vb, &bars[b]);
       if (spmv) {
-        bulk_copy(buf, rp + r0, rpb, &hs.bars[b]);
+        bulk_copy(buf, rp + r0, rpb, &bars[b]);
         if (cb) {
-          bulk_copy(buf + L::ci_off, ci + ka, cb, &hs.bars[b]);
-          bulk_copy(buf + L::v_off, v + ka, vvb, &hs.bars[b]);
+          bulk_copy(buf + L::ci_off, ci + ka, cb, &bars[b]);
+          bulk_copy(buf + L::v_off, v + ka, vvb, &bars[b]);
         }
       }
     };
-    if (threadIdx.x == 0)
-      for (int t = 0; t < S - 1 && t < nt; t++) issue(t);
-    for (int t = 0; t < nt; t++) {
-      if (threadIdx.x == 0 && t + S - 1 < nt) issue(t + S - 1);
-      const int b = t % S;
-      if (!mbar_wait(&hs.bars[b], (par >> b) & 1u)) {
-        atomicExch(abort_flag, 1);
-        hs.flag = 1;
-      }
+    if (lane == 0)
+      for (int j = 0; j < S - 1 && j < nj; j++) issue(j);
+    for (int j = 0; j < nj; j++) {
+      if (lane == 0 && j + S - 1 < nj) issue(j + S - 1);
+      const int b = j % S;
+      const bool got = __all_sync(0xffffffffu, mbar_wait(&bars[b], (par >> b) & 1u));
       par ^= 1u << b;
-      __syncthreads();
-      if (hs.flag) {  // leave; first let the prefetched tiles land (bounded)
-        for (int u = t + 1; u < nt && u < t + S; u++) {
-          mbar_wait(&hs.bars[u % S], (par >> (u % S)) & 1u);
+      if (!got) {  // raise the flag; let this warp's tiles in flight land (bounded), then leave
+        if (lane == 0) atomicExch(abort_flag, 1);
+        for (int u = j + 1; u < nj && u < j + S; u++) {
+          mbar_wait(&bars[u % S], (par >> (u % S)) & 1u);
           par ^= 1u << (u % S);
         }
-        ok = false;
         break;
       }
-      unsigned char *buf = smem + b * L::buf_bytes;
-      const int32_t r0 = base + t * R, rows = min(end, r0 + R) - r0;
+      const int t = warp + j * kWarps;
+      const int2 e0 = hs.tiles[t], e1 = hs.tiles[t + 1];
+      const int32_t r0 = e0.x, rows = e1.x - e0.x;
+      unsigned char *buf = wbuf + b * L::stage_bytes;
       const int32_t *rp_s = reinterpret_cast<const int32_t *>(buf);
       const int32_t *ci_s = reinterpret_cast<const int32_t *>(buf + L::ci_off);
       T *v_s = reinterpret_cast<T *>(buf + L::v_off);
       const T *slices = reinterpret_cast<const T *>(buf + L::vec_off);
-      int32_t ka = 0;
-      bool staged = false;
-      if (spmv) {
-        const int32_t k0 = hs.kb[t], k1 = hs.kb[t + 1];
-        ka = k0 & ~3;
-        const int32_t kbnd = (k1 + 3) & ~3;
-        staged = kbnd - ka <= L::kCapX;
-        if (staged) {
-#pragma unroll 4
-          for (int32_t k = k0 + threadIdx.x; k < k1; k += kThreads) v_s[k - ka] = v_s[k - ka] * ldv(xg + ci_s[k - ka]);
+      const int32_t k0 = e0.y, k1 = e1.y, ka = k0 & ~3;
+      const bool staged = spmv && ((k1 + 3) & ~3) - ka <= L::kCap;
+      if (staged) {  // the lanes' gathers are all issued before any product is stored
+        int32_t col[U];
+        T xv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const int32_t k = k0 + lane + u * 32;
+          col[u] = k < k1 ? ci_s[k - ka] : 0;
         }
-        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < U; u++) xv[u] = k0 + lane + u * 32 < k1 ? ldv(xg + col[u]) : T(0);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const int32_t k = k0 + lane + u * 32;
+          if (k < k1) v_s[k - ka] = v_s[k - ka] * xv[u];
+        }
+        __syncwarp();
       }
-      // row r goes to thread (r - lo) mod kThreads whatever R is, so each
-      // thread's running totals (and the block reductions) keep one order
-      const int rot = (t * R) & (kThreads - 1);
-      for (int i = (threadIdx.x - rot) & (kThreads - 1); i < rows; i += kThreads) {
+      if (lane < rows) {
         T acc = T(0);
         if (spmv) {
-          const int32_t a0 = rp_s[i], a1 = rp_s[i + 1];
-          if (staged) {
-            for (int32_t k = a0; k < a1; k++) acc = acc + v_s[k - ka];
+          const int32_t a0 = rp_s[lane], a1 = rp_s[lane + 1];
+          if (staged) {  // loads four ahead; the sum stays in index order
+            int32_t k = a0;
+            for (; k + 4 <= a1; k += 4) {
+              const T p0 = v_s[k - ka], p1 = v_s[k + 1 - ka], p2 = v_s[k + 2 - ka], p3 = v_s[k + 3 - ka];
+              acc = acc + p0;
+              acc = acc + p1;
+              acc = acc + p2;
+              acc = acc + p3;
+            }
+            for (; k < a1; k++) acc = acc + v_s[k - ka];
           } else {
             for (int32_t k = a0; k < a1; k++) acc = acc + (__ldg(v + k) * ldv(xg + __ldg(ci + k)));
           }
         }
-        epi(r0 + i, i, acc, slices);
+        epi(r0 + lane, lane, acc, slices);
       }
-      __syncthreads();
+      __syncwarp();
     }
+    __syncthreads();  // every warp is done with this batch's table entries
+    if (threadIdx.x == 0) hs.flag = *((volatile int32_t *)abort_flag);
+    __syncthreads();
+    if (hs.flag) return false;
   }
-  return ok;
+  return true;
 }
 
 // One shared staging area for every block reduction (a single allocation
@@ -355,11 +376,31 @@ __device__ __forceinline__ void reduce_partials(const double *partials, int stri
   double(&sh)[kMaxQ][kWarps] = reduction_scratch();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double v[Q];
+  // Every thread first issues its loads for up to kGroup slots x kWin
+  // partials at once (one L2 round trip instead of one per load), then sums
+  // each slot in block order.
+  constexpr int kGroup = 4, kWin = 4;
 #pragma unroll
-  for (int q = 0; q < Q; q++) {
-    double s = 0.0;
-    for (int b = threadIdx.x; b < nb; b += kThreads) s += ldv(partials + q * stride + b);
-    v[q] = s;
+  for (int q0 = 0; q0 < Q; q0 += kGroup) {
+    double val[kGroup][kWin];
+#pragma unroll
+    for (int g = 0; g < kGroup; g++)
+#pragma unroll
+      for (int k = 0; k < kWin; k++) {
+        const int b = threadIdx.x + k * kThreads;
+        val[g][k] = (q0 + g < Q && b < nb) ? ldv(partials + (q0 + g) * stride + b) : 0.0;
+      }
+#pragma unroll
+    for (int g = 0; g < kGroup; g++) {
+      if (q0 + g < Q) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < kWin; k++)
+          if (threadIdx.x + k * kThreads < nb) s += val[g][k];
+        for (int b = threadIdx.x + kWin * kThreads; b < nb; b += kThreads) s += ldv(partials + (q0 + g) * stride + b);
+        v[q0 + g] = s;
+      }
+    }
   }
 #pragma unroll
   for (int q = 0; q < Q; q++) {
@@ -662,10 +703,9 @@ __device__ void phase_init(const Args<T> &a, const Control &s, const Team &tm, T
 template <typename T>
 __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsigned char *smem, HotShared &hs,
                         unsigned &par) {
-  using L = HotLayout<T>;
   double v[1] = {0.0};
   int32_t lo, hi;
-  chunk(a.n, tm.nb, tm.rank, lo, hi);
+  chunk(a.ntiles_t, tm.nb, tm.rank, lo, hi);
   const T tau = (T)s.tau, w = (T)s.pend_w;
   const T *x = a.x[s.xc];
   T *xn_out = a.x[s.xc ^ 1];
@@ -681,20 +721,21 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
   bool ok;
   if (s.pend) {
     const T *vecs[6] = {x, a.sx, a.skty, a.c, a.l, a.u};
-    ok = hot_tiles<T>(lo, hi, a.rows_t, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], vecs, 6, smem, hs, par, &a.sync->abort,
-                      [&](int32_t j, int i, T kt, const T *sl) {
-                        constexpr int S = L::kRows;
+    ok = hot_tiles<T>(lo, hi, a.tiles_t, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], vecs, 6, smem, hs, par,
+                      &a.sync->abort, [&](int32_t j, int i, T kt, const T *sl) {
+                        constexpr int S = kWarpRows;
                         const T xj = sl[i], sx = sl[S + i], skt = sl[2 * S + i];
+                        const T cj = sl[3 * S + i], lj = sl[4 * S + i], uj = sl[5 * S + i];
                         a.kty[j] = kt;
                         a.sx[j] = (w * xj) + (T(1) * sx);
                         a.skty[j] = (w * kt) + (T(1) * skt);
-                        step(j, xj, kt, sl[3 * S + i], sl[4 * S + i], sl[5 * S + i]);
+                        step(j, xj, kt, cj, lj, uj);
                       });
   } else {
     const T *vecs[5] = {x, a.kty, a.c, a.l, a.u};
-    ok = hot_tiles<T>(lo, hi, L::kRows, nullptr, nullptr, nullptr, nullptr, vecs, 5, smem, hs, par, &a.sync->abort,
-                      [&](int32_t j, int i, T, const T *sl) {
-                        constexpr int S = L::kRows;
+    ok = hot_tiles<T>(lo, hi, a.tiles_t, nullptr, nullptr, nullptr, nullptr, vecs, 5, smem, hs, par,
+                      &a.sync->abort, [&](int32_t j, int i, T, const T *sl) {
+                        constexpr int S = kWarpRows;
                         step(j, sl[i], sl[S + i], sl[2 * S + i], sl[3 * S + i], sl[4 * S + i]);
                       });
   }
@@ -707,10 +748,9 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
 template <typename T>
 __device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsigned char *smem, HotShared &hs,
                         unsigned &par) {
-  using L = HotLayout<T>;
   double v[2] = {0.0, 0.0};
   int32_t lo, hi;
-  chunk(a.m, tm.nb, tm.rank, lo, hi);
+  chunk(a.ntiles_k, tm.nb, tm.rank, lo, hi);
   const T sigma = (T)s.sigma, w = (T)s.pend_w;
   const T *y = a.y[s.yc];
   const T *kx = a.kx[s.kxc];
@@ -726,20 +766,19 @@ __device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsi
     nv++;
   }
   const bool has_lo = a.ylo != nullptr;
-  const bool ok = hot_tiles<T>(lo, hi, a.rows_k, a.kp, a.kci, a.kv, (const T *)a.xbar, vecs, nv, smem, hs, par, &a.sync->abort,
-                               [&](int32_t r, int i, T kb, const T *sl) {
-    constexpr int S = L::kRows;
+  const bool ok = hot_tiles<T>(lo, hi, a.tiles_k, a.kp, a.kci, a.kv, (const T *)a.xbar, vecs, nv, smem, hs, par,
+                               &a.sync->abort, [&](int32_t r, int i, T kb, const T *sl) {
+    constexpr int S = kWarpRows;
     const T yr = sl[i], kxr = sl[S + i], qr = sl[2 * S + i];
+    const T syr = pend ? sl[3 * S + i] : T(0), skxr = pend ? sl[4 * S + i] : T(0);
+    const T lb = has_lo ? sl[iylo * S + i] : T(0);
     if (pend) {
-      a.sy[r] = (w * yr) + (T(1) * sl[3 * S + i]);
-      a.skx[r] = (w * kxr) + (T(1) * sl[4 * S + i]);
+      a.sy[r] = (w * yr) + (T(1) * syr);
+      a.skx[r] = (w * kxr) + (T(1) * skxr);
     }
     // ScalaKernels.dualStep (:100-118); around an anchor the cone is y >= -ya
     T yn = yr + (sigma * (qr - kb));
-    if (r >= a.neq) {
-      const T lb = has_lo ? sl[iylo * S + i] : T(0);
-      yn = yn > lb ? yn : lb;
-    }
+    if (r >= a.neq) yn = yn > lb ? yn : lb;
     y_out[r] = yn;
     kx_out[r] = (T(0.5) * kb) + (T(0.5) * kxr);
     const T dy = (T(1) * yn) + (T(-1) * yr);
@@ -1230,7 +1269,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksPerSm) pdhg_kernel(Args<T>
   const Team tm{(int)gridDim.x, (int)blockIdx.x, s_part};
   unsigned par = 0;  // mbarrier phase parity of the two tile buffers
   if (threadIdx.x == 0) {
-    for (int i = 0; i < HotLayout<T>::kStages; i++) mbar_init(&hs.bars[i], 1);
+    for (int i = 0; i < kWarps * kMaxStages; i++) mbar_init(&hs.bars[i], 1);
     fence_mbar_init();
   }
   load_control(a, snap);  // (syncs the block)
@@ -1324,7 +1363,7 @@ struct StateLayout {
 
 template <typename T>
 constexpr size_t dyn_smem() {
-  return std::max((size_t)dev::kTileCap * sizeof(T), dev::HotLayout<T>::total);
+  return std::max((size_t)dev::kTileCap * sizeof(T), dev::WarpLayout<T>::total);
 }
 
 template <typename T>
@@ -1350,23 +1389,46 @@ inline int team_blocks(int64_t n, int64_t m, int max_blocks) {
   return (int)std::min<int64_t>(max_blocks, (work + dev::kTileRows - 1) / dev::kTileRows);
 }
 
-// Rows per streamed tile: the largest power of two (<= 256) for which at most
-// 1/32 of the windows of that many rows, starting at a multiple of 4, hold
-// more nonzeros (rounded out to 16-byte granules) than one stage.  Fewer,
-// larger tiles beat fully staged small ones: a tile that does not fit reads
-// its indices and values from global memory instead.
+// The warp-tile table of a matrix with row pointers rp: tiles of at most
+// kWarpRows rows, starting at multiples of 4, grown 4 rows at a time while
+// their nonzeros (rounded out to 16-byte granules) fit one stage.  A group of
+// 4 rows that alone does not fit is a tile of its own, read unstaged.
+// Entries are (first row, first nonzero), closed by (rows, nnz).
 template <typename T>
-int32_t hot_rows(const std::vector<int32_t> &rp) {
-  const int64_t rows = (int64_t)rp.size() - 1, capx = dev::HotLayout<T>::kCapX;
-  for (int32_t R = dev::HotLayout<T>::kRows; R >= 4; R /= 2) {
-    int64_t over = 0, windows = 0;
-    for (int64_t r0 = 0; r0 < rows; r0 += 4, windows++) {
-      const int64_t r1 = std::min<int64_t>(rows, r0 + R);
-      if (((rp[r1] + 3) & ~3) - (rp[r0] & ~3) > capx) over++;
+std::vector<int2> warp_tile_table(const std::vector<int32_t> &rp) {
+  const int64_t rows = (int64_t)rp.size() - 1, cap = dev::WarpLayout<T>::kCap;
+  std::vector<int2> table;
+  table.reserve((size_t)(rows / 16 + 2));
+  int64_t r = 0;
+  while (r < rows) {
+    table.push_back(make_int2((int)r, rp[r]));
+    int64_t e = r;
+    while (e < rows && e - r < dev::kWarpRows) {
+      const int64_t e2 = std::min<int64_t>(rows, e + 4);
+      if (e > r && (((int64_t)rp[e2] + 3) & ~3) - (rp[r] & ~3) > cap) break;
+      e = e2;
     }
-    if (over * 32 <= windows) return R;
+    r = e;
   }
-  return 4;
+  table.push_back(make_int2((int)rows, rp[rows]));
+  return table;
+}
+
+// Builds (once per prepared problem and precision) and uploads the tables.
+template <typename T>
+int32_t ensure_tile_tables(PreparedLp &L, cudaStream_t s) {
+  const int w = sizeof(T) == 8;
+  if (L.ntiles[w][0] || (L.m == 0 && L.n == 0)) return PRIMA_OK;
+  const std::vector<int32_t> *rps[2] = {&L.h_kp, &L.h_tp};
+  for (int k = 0; k < 2; k++) {
+    const std::vector<int2> t = warp_tile_table<T>(*rps[k]);
+    int32_t rc;
+    if ((rc = L.b_tiles[w][k].reserve(t.size() * sizeof(int2)))) return rc;
+    PRIMA_CUDA_TRY(cudaMemcpyAsync(L.b_tiles[w][k].ptr, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+    PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
+    L.ntiles[w][k] = (int32_t)t.size() - 1;
+  }
+  return PRIMA_OK;
 }
 
 template <typename T>
@@ -1500,12 +1562,11 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   a.ctl = (dev::Control *)(base + S.ctl);
   a.sync = (dev::Sync *)(base + S.sync);
   a.prof = (dev::Prof *)(base + S.prof);
-  if (!L.hot_rows[w][0]) {
-    L.hot_rows[w][0] = hot_rows<T>(L.h_kp);
-    L.hot_rows[w][1] = hot_rows<T>(L.h_tp);
-  }
-  a.rows_k = L.hot_rows[w][0];
-  a.rows_t = L.hot_rows[w][1];
+  if ((rc = ensure_tile_tables<T>(L, s))) return rc;
+  a.tiles_k = (const int2 *)L.b_tiles[w][0].ptr;
+  a.tiles_t = (const int2 *)L.b_tiles[w][1].ptr;
+  a.ntiles_k = L.ntiles[w][0];
+  a.ntiles_t = L.ntiles[w][1];
   if (anchored) {
     a.anchored = 1;
     a.xa = (double *)(base + S.xa);
@@ -1624,8 +1685,8 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
     dev::Prof prof;
     PRIMA_CUDA_TRY(cudaMemcpy(&prof, a.prof, sizeof(prof), cudaMemcpyDeviceToHost));
     static const char *names[8] = {"init", "A", "B", "F", "R", "W", "-", "R2"};
-    std::fprintf(stderr, "[prima] blocks=%d rows=%d/%d trials=%lld decide %.2f us/barrier:", blocks, a.rows_k,
-                 a.rows_t, (long long)ctl.total_trials,
+    std::fprintf(stderr, "[prima] blocks=%d tiles=%d/%d trials=%lld decide %.2f us/barrier:", blocks, a.ntiles_k,
+                 a.ntiles_t, (long long)ctl.total_trials,
                  1e-3 * (double)prof.decide_ns / std::max<int64_t>(1, 2 * ctl.total_trials));
     for (int k = 0; k < 8; k++)
       if (prof.phase_count[k])

@@ -146,7 +146,8 @@ struct Args {
   double *xo, *yo, *rco;
   double *partials;  // [kMaxQ][max_blocks]
   int32_t max_blocks, anchored;
-  int32_t rows_k, rows_t;  // rows per streamed tile of K and of K' (their nonzeros fit the stage)
+  const int2 *tiles_k, *tiles_t;  // warp-tile tables of K and K': (first row, first nonzero), + a sentinel
+  int32_t ntiles_k, ntiles_t;
   Prof *prof;
   // Anchored (refinement) mode: the iterate is a correction (x^, y^) to an
   // FP64 anchor (xa, ya) whose exact products kxa = K xa, ktya = K'ya are
