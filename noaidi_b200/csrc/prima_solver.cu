@@ -147,7 +147,7 @@ template <>
 struct Warp<double> : WarpShape<PRIMA_WARP_F64_CAP, PRIMA_WARP_F64_STAGES> {};
 constexpr int kWarpRows = 32;     // rows per warp tile, at most (one per lane)
 constexpr int kWarpVec = 6;       // vector slices per tile, at most
-constexpr int kTileBatch = 256;   // tile-table entries a block stages at once
+constexpr int kSupBatch = 32;    // super-tiles (kWarps consecutive tiles) a block stages at once
 constexpr int kMaxStages = Warp<float>::kStages > Warp<double>::kStages ? Warp<float>::kStages : Warp<double>::kStages;
 
 template <typename T>
@@ -202,17 +202,21 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity) {
 
 struct HotShared {
   uint64_t bars[kWarps * kMaxStages];  // one mbarrier per warp stage
-  int2 tiles[kTileBatch + 1];          // (first row, first nonzero) of each tile
+  int2 tiles[kSupBatch * (kWarps + 1)];  // (first row, first nonzero): per super-tile, its tiles + the next
   int flag;
 };
 
-// The warp-tile engine over tiles [tlo, thi) of a table.  rp == nullptr: no
-// SpMV, vectors only.  epi(r, i, acc, slices) runs on lane i for row r of
+// The warp-tile engine over a table of ntiles tiles.  Tiles come in
+// super-tiles of kWarps consecutive tiles, one per warp; block `rank` of `nb`
+// takes super-tiles rank, rank + nb, rank + 2nb, ...  Every block thus gets
+// an even sample of the matrix (no block ends up with all of its heaviest
+// rows), and each thread's running totals keep a fixed order.  rp == nullptr:
+// no SpMV, vectors only.  epi(r, i, acc, slices) runs on lane i for row r of
 // the tile: acc is the row's product (an index-order sum from zero, as
 // csr_tiles), slices the tile's vector slices (stride kWarpRows).  Returns
 // false, uniformly over the block, when the team's abort flag is up.
 template <typename T, typename Epi>
-__device__ __forceinline__ bool hot_tiles(int32_t tlo, int32_t thi, const int2 *__restrict__ table,
+__device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, const int2 *__restrict__ table,
                                           const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
                                           const T *__restrict__ v, const T *xg, const T *const *vecs, int nv,
                                           unsigned char *smem, HotShared &hs, unsigned &par, int32_t *abort_flag,
@@ -224,15 +228,22 @@ __device__ __forceinline__ bool hot_tiles(int32_t tlo, int32_t thi, const int2 *
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char *wbuf = smem + (size_t)warp * L::warp_bytes;
   uint64_t *bars = hs.bars + warp * kMaxStages;
-  for (int32_t base = tlo; base < thi; base += kTileBatch) {
-    const int nt = min(kTileBatch, thi - base);
-    for (int t = threadIdx.x; t <= nt; t += kThreads) hs.tiles[t] = __ldg(table + base + t);
+  const int32_t nsup_all = (ntiles + kWarps - 1) / kWarps;
+  const int32_t nsup = rank < nsup_all ? (nsup_all - rank + nb - 1) / nb : 0;  // this block's super-tiles
+  for (int32_t jb = 0; jb < nsup; jb += kSupBatch) {
+    const int nsb = min(kSupBatch, nsup - jb);
+    for (int e = threadIdx.x; e < nsb * (kWarps + 1); e += kThreads) {
+      const int64_t t = (int64_t)(rank + (int64_t)(jb + e / (kWarps + 1)) * nb) * kWarps + e % (kWarps + 1);
+      hs.tiles[e] = __ldg(table + (t < ntiles ? t : ntiles));
+    }
     __syncthreads();
-    const int nj = nt > warp ? (nt - warp + kWarps - 1) / kWarps : 0;  // this warp's tiles: warp + j*kWarps
+    // this warp's tiles: super-tiles jb .. jb+nsb-1; only the very last one can be short
+    const int64_t last = (int64_t)(rank + (int64_t)(jb + nsb - 1) * nb) * kWarps + warp;
+    const int nj = nsb - (last < ntiles ? 0 : 1);
     auto issue = [&](int j) {  // lane 0
-      const int t = warp + j * kWarps, b = j % S;
+      const int b = j % S;
       unsigned char *buf = wbuf + b * L::stage_bytes;
-      const int2 e0 = hs.tiles[t], e1 = hs.tiles[t + 1];
+      const int2 e0 = hs.tiles[j * (kWarps + 1) + warp], e1 = hs.tiles[j * (kWarps + 1) + warp + 1];
       const int32_t r0 = e0.x, rows = e1.x - e0.x;
       const unsigned vb = ((unsigned)rows * (unsigned)sizeof(T) + 15u) & ~15u;
       unsigned total = (unsigned)nv * vb, rpb = 0, cb = 0, vvb = 0;
@@ -273,8 +284,7 @@ __device__ __forceinline__ bool hot_tiles(int32_t tlo, int32_t thi, const int2 *
         }
         break;
       }
-      const int t = warp + j * kWarps;
-      const int2 e0 = hs.tiles[t], e1 = hs.tiles[t + 1];
+      const int2 e0 = hs.tiles[j * (kWarps + 1) + warp], e1 = hs.tiles[j * (kWarps + 1) + warp + 1];
       const int32_t r0 = e0.x, rows = e1.x - e0.x;
       unsigned char *buf = wbuf + b * L::stage_bytes;
       const int32_t *rp_s = reinterpret_cast<const int32_t *>(buf);
@@ -704,8 +714,6 @@ template <typename T>
 __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsigned char *smem, HotShared &hs,
                         unsigned &par) {
   double v[1] = {0.0};
-  int32_t lo, hi;
-  chunk(a.ntiles_t, tm.nb, tm.rank, lo, hi);
   const T tau = (T)s.tau, w = (T)s.pend_w;
   const T *x = a.x[s.xc];
   T *xn_out = a.x[s.xc ^ 1];
@@ -721,7 +729,7 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
   bool ok;
   if (s.pend) {
     const T *vecs[6] = {x, a.sx, a.skty, a.c, a.l, a.u};
-    ok = hot_tiles<T>(lo, hi, a.tiles_t, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], vecs, 6, smem, hs, par,
+    ok = hot_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], vecs, 6, smem, hs, par,
                       &a.sync->abort, [&](int32_t j, int i, T kt, const T *sl) {
                         constexpr int S = kWarpRows;
                         const T xj = sl[i], sx = sl[S + i], skt = sl[2 * S + i];
@@ -733,7 +741,7 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
                       });
   } else {
     const T *vecs[5] = {x, a.kty, a.c, a.l, a.u};
-    ok = hot_tiles<T>(lo, hi, a.tiles_t, nullptr, nullptr, nullptr, nullptr, vecs, 5, smem, hs, par,
+    ok = hot_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, nullptr, nullptr, nullptr, nullptr, vecs, 5, smem, hs, par,
                       &a.sync->abort, [&](int32_t j, int i, T, const T *sl) {
                         constexpr int S = kWarpRows;
                         step(j, sl[i], sl[S + i], sl[2 * S + i], sl[3 * S + i], sl[4 * S + i]);
@@ -749,8 +757,6 @@ template <typename T>
 __device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsigned char *smem, HotShared &hs,
                         unsigned &par) {
   double v[2] = {0.0, 0.0};
-  int32_t lo, hi;
-  chunk(a.ntiles_k, tm.nb, tm.rank, lo, hi);
   const T sigma = (T)s.sigma, w = (T)s.pend_w;
   const T *y = a.y[s.yc];
   const T *kx = a.kx[s.kxc];
@@ -766,7 +772,7 @@ __device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsi
     nv++;
   }
   const bool has_lo = a.ylo != nullptr;
-  const bool ok = hot_tiles<T>(lo, hi, a.tiles_k, a.kp, a.kci, a.kv, (const T *)a.xbar, vecs, nv, smem, hs, par,
+  const bool ok = hot_tiles<T>(a.ntiles_k, tm.nb, tm.rank, a.tiles_k, a.kp, a.kci, a.kv, (const T *)a.xbar, vecs, nv, smem, hs, par,
                                &a.sync->abort, [&](int32_t r, int i, T kb, const T *sl) {
     constexpr int S = kWarpRows;
     const T yr = sl[i], kxr = sl[S + i], qr = sl[2 * S + i];
