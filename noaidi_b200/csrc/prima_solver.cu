@@ -113,55 +113,55 @@ __device__ __forceinline__ void csr_tiles(int32_t lo, int32_t hi, const int32_t 
 
 struct None {};
 
-// ---- TMA-prefetched warp tiles for the hot phases ------------------------
+// ---- TMA-staged tiles for the hot phases ----------------------------------
 //
-// Phases A and B cut the rows of K' (A) and K (B) into warp tiles: at most
-// 32 rows, starting at a multiple of 4, whose nonzeros (rounded out to
+// Phases A and B cut the rows of K' (A) and K (B) into tiles of at most
+// kRows rows, starting at a multiple of 4, whose nonzeros (rounded out to
 // 16-byte granules) fit one stage -- a table built once per matrix on the
-// host.  Each warp runs its own kStages-deep pipeline: its lane 0 streams a
-// tile's row pointers, column indices, values and up to six vector slices
-// into the warp's shared-memory stage with one-dimensional bulk copies
-// (cp.async.bulk, completion on the stage's mbarrier) while the warp works on
-// an earlier tile.  Warps never wait for one another inside a phase, so the
-// latency of one warp's gathers hides behind the other warps' streams.  Every
-// wait is bounded.
+// host.  Block `rank` of `nb` takes tiles rank, rank + nb, ..., so every
+// block gets an even sample of the matrix.  A tile's row pointers, column
+// indices, values and up to six vector slices arrive in one of kStages
+// shared-memory stages by one-dimensional bulk copies (cp.async.bulk,
+// completion on the stage's mbarrier).  Each warp then works on its own 32
+// rows of the tile with no block-wide synchronisation; the last warp to
+// finish with a stage refills it with the tile kStages further on.  A fast
+// warp thus runs ahead into the next stage while a slow one finishes, and
+// the copies for later tiles are in flight meanwhile.  Every wait is bounded.
 
-#ifndef PRIMA_WARP_F32_CAP
-#define PRIMA_WARP_F32_CAP 192
-#define PRIMA_WARP_F32_STAGES 2
+#ifndef PRIMA_HOT_F32_CAP
+#define PRIMA_HOT_F32_CAP 2048
+#define PRIMA_HOT_F32_STAGES 2
 #endif
-#ifndef PRIMA_WARP_F64_CAP
-#define PRIMA_WARP_F64_CAP 160
-#define PRIMA_WARP_F64_STAGES 2
+#ifndef PRIMA_HOT_F64_CAP
+#define PRIMA_HOT_F64_CAP 1024
+#define PRIMA_HOT_F64_STAGES 2
 #endif
 template <int C, int S>
-struct WarpShape {
-  static_assert(C % 32 == 0, "stage capacity in whole warps");
+struct HotShape {
   static constexpr int kCap = C, kStages = S;
 };
 template <typename T>
-struct Warp;
+struct Hot;
 template <>
-struct Warp<float> : WarpShape<PRIMA_WARP_F32_CAP, PRIMA_WARP_F32_STAGES> {};
+struct Hot<float> : HotShape<PRIMA_HOT_F32_CAP, PRIMA_HOT_F32_STAGES> {};
 template <>
-struct Warp<double> : WarpShape<PRIMA_WARP_F64_CAP, PRIMA_WARP_F64_STAGES> {};
-constexpr int kWarpRows = 32;     // rows per warp tile, at most (one per lane)
-constexpr int kWarpVec = 6;       // vector slices per tile, at most
-constexpr int kSupBatch = 32;    // super-tiles (kWarps consecutive tiles) a block stages at once
-constexpr int kMaxStages = Warp<float>::kStages > Warp<double>::kStages ? Warp<float>::kStages : Warp<double>::kStages;
+struct Hot<double> : HotShape<PRIMA_HOT_F64_CAP, PRIMA_HOT_F64_STAGES> {};
+constexpr int kHotRows = kThreads;  // rows per tile, at most: one per thread
+constexpr int kHotVec = 6;          // vector slices per tile, at most
+constexpr int kHotBatch = 128;      // tiles whose table entries a block stages at once
+constexpr int kMaxStages = Hot<float>::kStages > Hot<double>::kStages ? Hot<float>::kStages : Hot<double>::kStages;
 
 template <typename T>
-struct WarpLayout {
-  static constexpr int kCap = Warp<T>::kCap;  // staged nonzeros (16-byte rounded span)
-  static constexpr int kStages = Warp<T>::kStages;
-  static constexpr size_t rp_bytes = ((size_t)(kWarpRows + 1) * 4 + 15) / 16 * 16;
+struct HotLayout {
+  static constexpr int kCap = Hot<T>::kCap;  // staged nonzeros (16-byte rounded span)
+  static constexpr int kStages = Hot<T>::kStages;
+  static constexpr size_t rp_bytes = ((size_t)(kHotRows + 1) * 4 + 15) / 16 * 16;
   static constexpr size_t ci_off = rp_bytes;
   static constexpr size_t v_off = ci_off + (size_t)kCap * 4;
   static constexpr size_t vec_off = (v_off + (size_t)kCap * sizeof(T) + 15) / 16 * 16;
-  static constexpr size_t vec_stride = (size_t)kWarpRows * sizeof(T);
-  static constexpr size_t stage_bytes = (vec_off + kWarpVec * vec_stride + 15) / 16 * 16;
-  static constexpr size_t warp_bytes = kStages * stage_bytes;
-  static constexpr size_t total = kWarps * warp_bytes;
+  static constexpr size_t vec_stride = (size_t)kHotRows * sizeof(T);
+  static constexpr size_t stage_bytes = (vec_off + kHotVec * vec_stride + 127) / 128 * 128;
+  static constexpr size_t total = kStages * stage_bytes;
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -201,49 +201,43 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity) {
 }
 
 struct HotShared {
-  uint64_t bars[kWarps * kMaxStages];  // one mbarrier per warp stage
-  int2 tiles[kSupBatch * (kWarps + 1)];  // (first row, first nonzero): per super-tile, its tiles + the next
+  uint64_t bars[kMaxStages];       // stage full: the tile's bytes have landed
+  unsigned done[kMaxStages];       // warps finished with the stage's tile
+  int2 tiles[2 * kHotBatch];       // per tile of the batch: (first row, first nonzero) of it and of the next
+  int issued;                      // tiles of the batch issued so far
   int flag;
 };
 
-// The warp-tile engine over a table of ntiles tiles.  Tiles come in
-// super-tiles of kWarps consecutive tiles, one per warp; block `rank` of `nb`
-// takes super-tiles rank, rank + nb, rank + 2nb, ...  Every block thus gets
-// an even sample of the matrix (no block ends up with all of its heaviest
-// rows), and each thread's running totals keep a fixed order.  rp == nullptr:
-// no SpMV, vectors only.  epi(r, i, acc, slices) runs on lane i for row r of
-// the tile: acc is the row's product (an index-order sum from zero, as
-// csr_tiles), slices the tile's vector slices (stride kWarpRows).  Returns
-// false, uniformly over the block, when the team's abort flag is up.
+// The tile engine over a table of ntiles tiles (see above).  rp == nullptr:
+// no SpMV, vectors only.  epi(r, i, acc, slices) runs on the thread of row i
+// of the tile (row r of the matrix): acc is the row's product (an
+// index-order sum from zero, as csr_tiles), slices the tile's vector slices
+// (stride kHotRows).  Returns false, uniformly over the block, when the
+// team's abort flag is up.
 template <typename T, typename Epi>
 __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, const int2 *__restrict__ table,
                                           const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
                                           const T *__restrict__ v, const T *xg, const T *const *vecs, int nv,
                                           unsigned char *smem, HotShared &hs, unsigned &par, int32_t *abort_flag,
                                           Epi &&epi) {
-  using L = WarpLayout<T>;
+  using L = HotLayout<T>;
   constexpr int S = L::kStages;
-  constexpr int U = L::kCap / 32;  // gathers per lane per tile, at most
   const bool spmv = rp != nullptr;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned char *wbuf = smem + (size_t)warp * L::warp_bytes;
-  uint64_t *bars = hs.bars + warp * kMaxStages;
-  const int32_t nsup_all = (ntiles + kWarps - 1) / kWarps;
-  const int32_t nsup = rank < nsup_all ? (nsup_all - rank + nb - 1) / nb : 0;  // this block's super-tiles
-  for (int32_t jb = 0; jb < nsup; jb += kSupBatch) {
-    const int nsb = min(kSupBatch, nsup - jb);
-    for (int e = threadIdx.x; e < nsb * (kWarps + 1); e += kThreads) {
-      const int64_t t = (int64_t)(rank + (int64_t)(jb + e / (kWarps + 1)) * nb) * kWarps + e % (kWarps + 1);
-      hs.tiles[e] = __ldg(table + (t < ntiles ? t : ntiles));
+  const int32_t mine = rank < ntiles ? (ntiles - rank + nb - 1) / nb : 0;  // this block's tiles
+  for (int32_t jb = 0; jb < mine; jb += kHotBatch) {
+    const int nj = min(kHotBatch, mine - jb);
+    for (int e = threadIdx.x; e < 2 * nj; e += kThreads) {
+      const int64_t t = rank + (int64_t)(jb + (e >> 1)) * nb + (e & 1);
+      hs.tiles[e] = __ldg(table + t);
     }
+    if (threadIdx.x < S) hs.done[threadIdx.x] = 0;
+    if (threadIdx.x == 0) hs.issued = 0;
     __syncthreads();
-    // this warp's tiles: super-tiles jb .. jb+nsb-1; only the very last one can be short
-    const int64_t last = (int64_t)(rank + (int64_t)(jb + nsb - 1) * nb) * kWarps + warp;
-    const int nj = nsb - (last < ntiles ? 0 : 1);
-    auto issue = [&](int j) {  // lane 0
+    auto issue = [&](int j) {  // one thread
       const int b = j % S;
-      unsigned char *buf = wbuf + b * L::stage_bytes;
-      const int2 e0 = hs.tiles[j * (kWarps + 1) + warp], e1 = hs.tiles[j * (kWarps + 1) + warp + 1];
+      unsigned char *buf = smem + b * L::stage_bytes;
+      const int2 e0 = hs.tiles[2 * j], e1 = hs.tiles[2 * j + 1];
       const int32_t r0 = e0.x, rows = e1.x - e0.x;
       const unsigned vb = ((unsigned)rows * (unsigned)sizeof(T) + 15u) & ~15u;
       unsigned total = (unsigned)nv * vb, rpb = 0, cb = 0, vvb = 0;
@@ -259,81 +253,88 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
         total += rpb + cb + vvb;
       }
       fence_proxy_async();
-      mbar_expect_tx(&bars[b], total);
-      for (int i = 0; i < nv; i++) bulk_copy(buf + L::vec_off + i * L::vec_stride, vecs[i] + r0, vb, &bars[b]);
+      hs.issued = j + 1;
+      mbar_expect_tx(&hs.bars[b], total);
+      for (int i = 0; i < nv; i++) bulk_copy(buf + L::vec_off + i * L::vec_stride, vecs[i] + r0, vb, &hs.bars[b]);
       if (spmv) {
-        bulk_copy(buf, rp + r0, rpb, &bars[b]);
+        bulk_copy(buf, rp + r0, rpb, &hs.bars[b]);
         if (cb) {
-          bulk_copy(buf + L::ci_off, ci + ka, cb, &bars[b]);
-          bulk_copy(buf + L::v_off, v + ka, vvb, &bars[b]);
+          bulk_copy(buf + L::ci_off, ci + ka, cb, &hs.bars[b]);
+          bulk_copy(buf + L::v_off, v + ka, vvb, &hs.bars[b]);
         }
       }
     };
-    if (lane == 0)
-      for (int j = 0; j < S - 1 && j < nj; j++) issue(j);
-    for (int j = 0; j < nj; j++) {
-      if (lane == 0 && j + S - 1 < nj) issue(j + S - 1);
+    if (threadIdx.x == 0)
+      for (int j = 0; j < S && j < nj; j++) issue(j);
+    __syncthreads();
+    int j = 0;
+    for (; j < nj; j++) {
       const int b = j % S;
-      const bool got = __all_sync(0xffffffffu, mbar_wait(&bars[b], (par >> b) & 1u));
-      par ^= 1u << b;
-      if (!got) {  // raise the flag; let this warp's tiles in flight land (bounded), then leave
+      if (!__all_sync(0xffffffffu, mbar_wait(&hs.bars[b], (par >> b) & 1u))) {
         if (lane == 0) atomicExch(abort_flag, 1);
-        for (int u = j + 1; u < nj && u < j + S; u++) {
-          mbar_wait(&bars[u % S], (par >> (u % S)) & 1u);
-          par ^= 1u << (u % S);
-        }
         break;
       }
-      const int2 e0 = hs.tiles[j * (kWarps + 1) + warp], e1 = hs.tiles[j * (kWarps + 1) + warp + 1];
+      par ^= 1u << b;
+      const int2 e0 = hs.tiles[2 * j], e1 = hs.tiles[2 * j + 1];
       const int32_t r0 = e0.x, rows = e1.x - e0.x;
-      unsigned char *buf = wbuf + b * L::stage_bytes;
+      const unsigned char *buf = smem + b * L::stage_bytes;
       const int32_t *rp_s = reinterpret_cast<const int32_t *>(buf);
       const int32_t *ci_s = reinterpret_cast<const int32_t *>(buf + L::ci_off);
-      T *v_s = reinterpret_cast<T *>(buf + L::v_off);
+      const T *v_s = reinterpret_cast<const T *>(buf + L::v_off);
       const T *slices = reinterpret_cast<const T *>(buf + L::vec_off);
-      const int32_t k0 = e0.y, k1 = e1.y, ka = k0 & ~3;
-      const bool staged = spmv && ((k1 + 3) & ~3) - ka <= L::kCap;
-      if (staged) {  // the lanes' gathers are all issued before any product is stored
-        int32_t col[U];
-        T xv[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-          const int32_t k = k0 + lane + u * 32;
-          col[u] = k < k1 ? ci_s[k - ka] : 0;
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) xv[u] = k0 + lane + u * 32 < k1 ? ldv(xg + col[u]) : T(0);
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-          const int32_t k = k0 + lane + u * 32;
-          if (k < k1) v_s[k - ka] = v_s[k - ka] * xv[u];
-        }
-        __syncwarp();
-      }
-      if (lane < rows) {
+      const int32_t ka = e0.y & ~3;
+      const bool staged = spmv && ((e1.y + 3) & ~3) - ka <= L::kCap;
+      const int i = threadIdx.x;
+      if (i < rows) {
         T acc = T(0);
         if (spmv) {
-          const int32_t a0 = rp_s[lane], a1 = rp_s[lane + 1];
-          if (staged) {  // loads four ahead; the sum stays in index order
+          const int32_t a0 = rp_s[i], a1 = rp_s[i + 1];
+          if (staged) {  // four gathers in flight; the sum stays in index order
             int32_t k = a0;
             for (; k + 4 <= a1; k += 4) {
-              const T p0 = v_s[k - ka], p1 = v_s[k + 1 - ka], p2 = v_s[k + 2 - ka], p3 = v_s[k + 3 - ka];
-              acc = acc + p0;
-              acc = acc + p1;
-              acc = acc + p2;
-              acc = acc + p3;
+              const int32_t c0 = ci_s[k - ka], c1 = ci_s[k + 1 - ka], c2 = ci_s[k + 2 - ka], c3 = ci_s[k + 3 - ka];
+              const T x0 = ldv(xg + c0), x1 = ldv(xg + c1), x2 = ldv(xg + c2), x3 = ldv(xg + c3);
+              acc = acc + (v_s[k - ka] * x0);
+              acc = acc + (v_s[k + 1 - ka] * x1);
+              acc = acc + (v_s[k + 2 - ka] * x2);
+              acc = acc + (v_s[k + 3 - ka] * x3);
             }
-            for (; k < a1; k++) acc = acc + v_s[k - ka];
+            const int rem = a1 - k;
+            if (rem > 0) {
+              const int32_t c0 = ci_s[k - ka];
+              const int32_t c1 = rem > 1 ? ci_s[k + 1 - ka] : c0, c2 = rem > 2 ? ci_s[k + 2 - ka] : c0;
+              const T x0 = ldv(xg + c0), x1 = ldv(xg + c1), x2 = ldv(xg + c2);
+              acc = acc + (v_s[k - ka] * x0);
+              if (rem > 1) acc = acc + (v_s[k + 1 - ka] * x1);
+              if (rem > 2) acc = acc + (v_s[k + 2 - ka] * x2);
+            }
           } else {
             for (int32_t k = a0; k < a1; k++) acc = acc + (__ldg(v + k) * ldv(xg + __ldg(ci + k)));
           }
         }
-        epi(r0 + lane, lane, acc, slices);
+        epi(r0 + i, i, acc, slices);
       }
+      // the last warp done with this stage refills it with the tile S further on
       __syncwarp();
+      if (lane == 0) {
+        __threadfence_block();
+        if (atomicAdd(&hs.done[b], 1u) == (unsigned)(kWarps - 1)) {
+          __threadfence_block();
+          hs.done[b] = 0;
+          if (j + S < nj) issue(j + S);
+        }
+      }
     }
-    __syncthreads();  // every warp is done with this batch's table entries
-    if (threadIdx.x == 0) hs.flag = *((volatile int32_t *)abort_flag);
+    // leave the batch: every warp is past the loop; then let any copies still
+    // in flight land (bounded) before the stages or the table are reused
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      hs.flag = *((volatile int32_t *)abort_flag);
+      for (int u = j; u < hs.issued; u++) {  // only after an abort: tiles issued but never consumed
+        mbar_wait(&hs.bars[u % S], (par >> (u % S)) & 1u);
+        par ^= 1u << (u % S);
+      }
+    }
     __syncthreads();
     if (hs.flag) return false;
   }
@@ -731,7 +732,7 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
     const T *vecs[6] = {x, a.sx, a.skty, a.c, a.l, a.u};
     ok = hot_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], vecs, 6, smem, hs, par,
                       &a.sync->abort, [&](int32_t j, int i, T kt, const T *sl) {
-                        constexpr int S = kWarpRows;
+                        constexpr int S = kHotRows;
                         const T xj = sl[i], sx = sl[S + i], skt = sl[2 * S + i];
                         const T cj = sl[3 * S + i], lj = sl[4 * S + i], uj = sl[5 * S + i];
                         a.kty[j] = kt;
@@ -743,7 +744,7 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
     const T *vecs[5] = {x, a.kty, a.c, a.l, a.u};
     ok = hot_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, nullptr, nullptr, nullptr, nullptr, vecs, 5, smem, hs, par,
                       &a.sync->abort, [&](int32_t j, int i, T, const T *sl) {
-                        constexpr int S = kWarpRows;
+                        constexpr int S = kHotRows;
                         step(j, sl[i], sl[S + i], sl[2 * S + i], sl[3 * S + i], sl[4 * S + i]);
                       });
   }
@@ -774,7 +775,7 @@ __device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsi
   const bool has_lo = a.ylo != nullptr;
   const bool ok = hot_tiles<T>(a.ntiles_k, tm.nb, tm.rank, a.tiles_k, a.kp, a.kci, a.kv, (const T *)a.xbar, vecs, nv, smem, hs, par,
                                &a.sync->abort, [&](int32_t r, int i, T kb, const T *sl) {
-    constexpr int S = kWarpRows;
+    constexpr int S = kHotRows;
     const T yr = sl[i], kxr = sl[S + i], qr = sl[2 * S + i];
     const T syr = pend ? sl[3 * S + i] : T(0), skxr = pend ? sl[4 * S + i] : T(0);
     const T lb = has_lo ? sl[iylo * S + i] : T(0);
@@ -1275,7 +1276,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksPerSm) pdhg_kernel(Args<T>
   const Team tm{(int)gridDim.x, (int)blockIdx.x, s_part};
   unsigned par = 0;  // mbarrier phase parity of the two tile buffers
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kWarps * kMaxStages; i++) mbar_init(&hs.bars[i], 1);
+    for (int i = 0; i < kMaxStages; i++) mbar_init(&hs.bars[i], 1);
     fence_mbar_init();
   }
   load_control(a, snap);  // (syncs the block)
@@ -1369,7 +1370,7 @@ struct StateLayout {
 
 template <typename T>
 constexpr size_t dyn_smem() {
-  return std::max((size_t)dev::kTileCap * sizeof(T), dev::WarpLayout<T>::total);
+  return std::max((size_t)dev::kTileCap * sizeof(T), dev::HotLayout<T>::total);
 }
 
 template <typename T>
@@ -1395,21 +1396,21 @@ inline int team_blocks(int64_t n, int64_t m, int max_blocks) {
   return (int)std::min<int64_t>(max_blocks, (work + dev::kTileRows - 1) / dev::kTileRows);
 }
 
-// The warp-tile table of a matrix with row pointers rp: tiles of at most
-// kWarpRows rows, starting at multiples of 4, grown 4 rows at a time while
+// The tile table of a matrix with row pointers rp: tiles of at most
+// kHotRows rows, starting at multiples of 4, grown 4 rows at a time while
 // their nonzeros (rounded out to 16-byte granules) fit one stage.  A group of
 // 4 rows that alone does not fit is a tile of its own, read unstaged.
 // Entries are (first row, first nonzero), closed by (rows, nnz).
 template <typename T>
-std::vector<int2> warp_tile_table(const std::vector<int32_t> &rp) {
-  const int64_t rows = (int64_t)rp.size() - 1, cap = dev::WarpLayout<T>::kCap;
+std::vector<int2> tile_table(const std::vector<int32_t> &rp) {
+  const int64_t rows = (int64_t)rp.size() - 1, cap = dev::HotLayout<T>::kCap;
   std::vector<int2> table;
   table.reserve((size_t)(rows / 16 + 2));
   int64_t r = 0;
   while (r < rows) {
     table.push_back(make_int2((int)r, rp[r]));
     int64_t e = r;
-    while (e < rows && e - r < dev::kWarpRows) {
+    while (e < rows && e - r < dev::kHotRows) {
       const int64_t e2 = std::min<int64_t>(rows, e + 4);
       if (e > r && (((int64_t)rp[e2] + 3) & ~3) - (rp[r] & ~3) > cap) break;
       e = e2;
@@ -1427,7 +1428,7 @@ int32_t ensure_tile_tables(PreparedLp &L, cudaStream_t s) {
   if (L.ntiles[w][0] || (L.m == 0 && L.n == 0)) return PRIMA_OK;
   const std::vector<int32_t> *rps[2] = {&L.h_kp, &L.h_tp};
   for (int k = 0; k < 2; k++) {
-    const std::vector<int2> t = warp_tile_table<T>(*rps[k]);
+    const std::vector<int2> t = tile_table<T>(*rps[k]);
     int32_t rc;
     if ((rc = L.b_tiles[w][k].reserve(t.size() * sizeof(int2)))) return rc;
     PRIMA_CUDA_TRY(cudaMemcpyAsync(L.b_tiles[w][k].ptr, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, s));

@@ -6,8 +6,12 @@ and the validation ladder, in FP64 (ScalaKernels semantics) and FP32
 Tolerances: status identical; objective within 1e-8 relative of the oracle's
 FP64 answer at eps = 1e-9 (the ladder's worst-gap bound).  Iteration counts:
 the device reduces in a fixed tree and evaluates pow/exp/log with CUDA's
-libm, so a trajectory may shift by whole evaluation periods; the tiny
-fixtures, where neither can change a bit, must match exactly."""
+libm, so its trajectory can differ from the oracle's in the last bit.  The
+tiny fixtures, where neither can change a bit, must match exactly.  The
+others are chaotic in the last bit -- the oracle itself moves by up to
+several times when one objective coefficient moves by one ulp -- so their
+count must lie within that spread (tests/golden/ladder_envelope.json, made by
+make_ladder_envelope.py), widened by a quarter."""
 import ctypes
 import json
 import math
@@ -24,6 +28,7 @@ from tests import lp_fixtures as F
 pytestmark = pytest.mark.gpu
 
 PINS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_pins.json")))
+ENVELOPE = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ladder_envelope.json")))
 P9 = PdhgParams(eps_abs=1e-9, eps_rel=1e-9, max_iterations=500_000)
 LADDER = F.ladder()
 EXACT = {"tiny-lower-bound", "product-mix", "equality-split", "degenerate", "free-sign", "range-row",
@@ -46,7 +51,9 @@ def test_ladder_fp64_matches_oracle(entry):
     if entry.name in EXACT:
         assert (got.iterations, got.restarts) == (ref.iterations, ref.restarts)
     else:
-        assert abs(got.iterations - ref.iterations) <= max(128, 0.25 * ref.iterations)
+        env = ENVELOPE[entry.name]
+        lo, hi = min(env["perturbed"] + [ref.iterations]), max(env["perturbed"] + [ref.iterations])
+        assert lo / 1.25 - 128 <= got.iterations <= hi * 1.25 + 128, (got.iterations, lo, hi)
 
 
 @pytest.mark.parametrize("entry", LADDER[:10], ids=lambda e: e.name)
