@@ -223,7 +223,7 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
   using L = HotLayout<T>;
   constexpr int S = L::kStages;
   const bool spmv = rp != nullptr;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31;
   const int32_t mine = rank < ntiles ? (ntiles - rank + nb - 1) / nb : 0;  // this block's tiles
   for (int32_t jb = 0; jb < mine; jb += kHotBatch) {
     const int nj = min(kHotBatch, mine - jb);
