@@ -325,7 +325,7 @@ def main():
 # DRAM bytes (read + write) per step-size trial of pdhg_kernel<float> on this
 # workload, from an ncu capture of a bounded run of the same instance; None
 # until measured.
-TRAFFIC_BYTES_PER_TRIAL = 151.3e6
+TRAFFIC_BYTES_PER_TRIAL = 148.3e6
 
 if __name__ == "__main__":
     main()
