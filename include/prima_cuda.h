@@ -241,6 +241,16 @@ int32_t prima_pdhg_solve_batch(prima_handle ctx, int32_t count, const prima_lp *
                                double *const *primal_out, double *const *dual_out,
                                double *const *reduced_costs_out, prima_solution_info *infos);
 
+/* MixedPrecision.solve for `count` independent LPs, as by prima_mixed_solve,
+ * with each pass run for all instances in one persistent launch: the reduced
+ * FP32 pass, then the FP32 refinement finishes, then any FP64 finishes.
+ * Output arrays are per instance; any pointer array (or entry) may be NULL. */
+int32_t prima_mixed_solve_batch(prima_handle ctx, int32_t count, const prima_lp *lps, const prima_params *params,
+                                const prima_mixed_params *mixed, const volatile int32_t *cancel,
+                                double *const *primal_out, double *const *dual_out,
+                                double *const *reduced_costs_out, prima_solution_info *infos,
+                                prima_mixed_info *mixed_infos);
+
 /* ---- device-resident problems ---------------------------------------------
  * A problem uploaded and equilibrated once, then solved any number of times
  * (warm-started passes, mixed-precision passes, repeated sweeps) without

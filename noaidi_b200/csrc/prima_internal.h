@@ -137,6 +137,7 @@ struct Ctx {
   int32_t *cancel_mapped = nullptr;  // pinned + mapped: cancel flag seen by the device
   int32_t *cancel_mapped_dev = nullptr;
   DeviceBuffer solver_arena;   // buffers of the coarse solvers, reused across solves
+  DeviceBuffer batch_arena;    // state, arguments and queue of a batch launch
   PreparedLp scratch_lp;       // the problem of a one-shot solve call
   std::unordered_map<int64_t, std::unique_ptr<PreparedLp>> problems;
 };

@@ -1149,7 +1149,10 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
       break;
     }
     default:  // PH_W
-      if (threadIdx.x == 0) c.phase = PH_DONE;
+      if (threadIdx.x == 0) {
+        c.phase = PH_DONE;
+        c.t_end = global_timer_ns();
+      }
   }
 }
 
@@ -1204,6 +1207,7 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
       const uint64_t t1 = global_timer_ns();
       a.prof->decide_ns += t1 - t0;
       a.prof->t_release = t1;
+      if (snap.phase == PH_DONE && a.queue) a.team_next[a.team] = atomicAdd(a.queue, 1);
     }
     __syncthreads();
     return true;
@@ -1233,6 +1237,7 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     }
     __syncthreads();
     if (phase != PH_A) publish_control(a, snap);
+    if (threadIdx.x == 0 && snap.phase == PH_DONE && a.queue) a.team_next[a.team] = atomicAdd(a.queue, 1);
     if (threadIdx.x == 0) {
       const uint64_t t1 = global_timer_ns();
       a.prof->decide_ns += t1 - s_t0;
@@ -1266,20 +1271,14 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
   return s_ok;
 }
 
+// One whole solve by one team: the phase machine from the Control record the
+// host prepared to PH_DONE.  False: the team's abort flag went up.
 template <typename T>
-__global__ void __launch_bounds__(kThreads, kMinBlocksPerSm) pdhg_kernel(Args<T> a) {
-  __shared__ Control snap;
-  __shared__ double s_part[kMaxQ];
-  __shared__ HotShared hs;
-  extern __shared__ __align__(128) unsigned char s_dyn[];
+__device__ __forceinline__ bool run_solve(const Args<T> &a, const Team &tm, Control &snap, HotShared &hs,
+                                          unsigned &par, unsigned char *s_dyn) {
   T *s_prod = reinterpret_cast<T *>(s_dyn);
-  const Team tm{(int)gridDim.x, (int)blockIdx.x, s_part};
-  unsigned par = 0;  // mbarrier phase parity of the two tile buffers
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < kMaxStages; i++) mbar_init(&hs.bars[i], 1);
-    fence_mbar_init();
-  }
   load_control(a, snap);  // (syncs the block)
+  bool alive = true;
   for (;;) {
     const int ph = snap.phase;
     if (ph == PH_DONE) break;
@@ -1295,9 +1294,72 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksPerSm) pdhg_kernel(Args<T>
       default: break;
     }
     (void)ok;  // a failed tile wait has raised the team's abort flag; the barrier sees it
-    if (!barrier_decide(a, snap, ph, tm)) break;
+    if (!barrier_decide(a, snap, ph, tm)) {
+      alive = false;
+      break;
+    }
   }
   if (tm.nb == 1) publish_control(a, snap);  // the host reads the final record
+  return alive;
+}
+
+__device__ __forceinline__ void init_stages(HotShared &hs) {
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kMaxStages; i++) mbar_init(&hs.bars[i], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, kMinBlocksPerSm) pdhg_kernel(Args<T> a) {
+  __shared__ Control snap;
+  __shared__ double s_part[kMaxQ];
+  __shared__ HotShared hs;
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  const Team tm{(int)gridDim.x, (int)blockIdx.x, s_part};
+  unsigned par = 0;  // mbarrier phase parity of the tile stages
+  init_stages(hs);
+  run_solve(a, tm, snap, hs, par, s_dyn);
+}
+
+// Many independent LPs in one launch: the grid is cut into teams of tb
+// blocks; team k starts with instance k (instances come largest first) and,
+// whenever it finishes one, takes the next index from a shared queue (the
+// deciding block of the finishing barrier takes it for the whole team).  Each
+// instance has its own Control, Sync and state; a team runs exactly the
+// single-solve phase machine on it.
+template <typename T>
+__global__ void __launch_bounds__(kThreads, kMinBlocksPerSm)
+    pdhg_batch_kernel(const Args<T> *__restrict__ args, int count, int tb, int32_t *queue, int32_t *team_next) {
+  __shared__ Control snap;
+  __shared__ double s_part[kMaxQ];
+  __shared__ HotShared hs;
+  __shared__ Args<T> s_a;
+  __shared__ int s_inst;
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  const int team = (int)blockIdx.x / tb;
+  const Team tm{tb, (int)blockIdx.x % tb, s_part};
+  unsigned par = 0;
+  init_stages(hs);
+  int inst = team;
+  while (inst < count) {
+    const unsigned *src = reinterpret_cast<const unsigned *>(args + inst);
+    unsigned *dst = reinterpret_cast<unsigned *>(&s_a);
+    for (int i = threadIdx.x; i < (int)(sizeof(Args<T>) / 4); i += kThreads) dst[i] = __ldg(src + i);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_a.queue = queue;
+      s_a.team_next = team_next;
+      s_a.team = team;
+    }
+    __syncthreads();
+    if (!run_solve(s_a, tm, snap, hs, par, s_dyn)) break;
+    if (threadIdx.x == 0) s_inst = __ldcg(team_next + team);
+    __syncthreads();
+    inst = s_inst;
+    __syncthreads();
+  }
 }
 
 }  // namespace dev
@@ -1469,32 +1531,47 @@ int32_t check_warm(const PreparedLp &L, const prima_warm_start *w) {
   return PRIMA_OK;
 }
 
-// Pdhg.Solve on a prepared problem: initialise (Pdhg.scala:250-309) on the
-// host -- the opening step, primal weight and the projected start point --
-// then the whole iteration in one cooperative launch.
+// One solve in flight: the prepared problem, the caller's request and the
+// device-side arguments built for it.
 template <typename T>
-int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::time_point t_start) {
-  const prima_params *p = req.params;
+struct Job {
+  PreparedLp *L = nullptr;
+  SolveRequest req{};
+  Clock::time_point t0;
+  dev::Args<T> a{};
+  double setup_ms = 0.0;
+};
+
+// Everything a solve needs on the device before its launch that does not
+// depend on where its state lives: the precision copies, the FP64 copies for
+// anchored mode, the tile tables.
+template <typename T>
+int32_t prepare_job(Ctx *c, Job<T> &j) {
   int32_t rc;
-  if ((rc = check_warm(L, req.warm))) return rc;
+  if ((rc = check_warm(*j.L, j.req.warm))) return rc;
+  PreparedLp &L = *j.L;
+  if ((rc = L.materialise<T>(c->stream))) return rc;
+  if (j.req.anchored && (rc = L.materialise<double>(c->stream))) return rc;
+  return ensure_tile_tables<T>(L, c->stream);
+}
+
+// Pdhg.Solve's initialise (Pdhg.scala:250-309) on the host -- the opening
+// step, primal weight and the projected start point -- and the Args, Control
+// and Sync records, with the iterate state at `base` laid out as S.
+template <typename T>
+int32_t setup_job(Ctx *c, Job<T> &j, char *base, const StateLayout<T> &S, int blocks) {
+  PreparedLp &L = *j.L;
+  const SolveRequest &req = j.req;
+  const prima_params *p = req.params;
   cudaStream_t s = c->stream;
-  if ((rc = L.materialise<T>(s))) return rc;
   const int32_t n = L.n, m = L.m, neq = L.neq;
+  const bool anchored = req.anchored;
 
   const double bound = L.scaled_spectral_bound;
   double step = bound > 0.0 ? 1.0 / bound : 1.0;
   double weight = (L.scaled_c_norm > 0.0 && L.scaled_q_norm > 0.0) ? L.scaled_c_norm / L.scaled_q_norm : 1.0;
   if (req.warm && !std::isnan(req.warm->step_size)) step = req.warm->step_size;
   if (req.warm && !std::isnan(req.warm->primal_weight)) weight = req.warm->primal_weight;
-
-  int max_blocks = 0;
-  if ((rc = max_coresident_blocks<T>(c, &max_blocks))) return rc;
-  const int blocks = team_blocks(n, m, max_blocks);
-  const bool anchored = req.anchored;
-  if (anchored && (rc = L.materialise<double>(s))) return rc;
-  const StateLayout<T> S(n, m, blocks, anchored);
-  if ((rc = c->solver_arena.reserve(S.bytes))) return rc;
-  char *base = (char *)c->solver_arena.ptr;
 
   // start point: zero (or the warm start scaled in), projected into the box;
   // in anchored mode it becomes the FP64 anchor and the correction is zero
@@ -1526,7 +1603,7 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
     PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
   }
 
-  dev::Args<T> a;
+  dev::Args<T> &a = j.a;
   std::memset(&a, 0, sizeof(a));
   a.n = n;
   a.m = m;
@@ -1569,7 +1646,6 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   a.ctl = (dev::Control *)(base + S.ctl);
   a.sync = (dev::Sync *)(base + S.sync);
   a.prof = (dev::Prof *)(base + S.prof);
-  if ((rc = ensure_tile_tables<T>(L, s))) return rc;
   a.tiles_k = (const int2 *)L.b_tiles[w][0].ptr;
   a.tiles_t = (const int2 *)L.b_tiles[w][1].ptr;
   a.ntiles_k = L.ntiles[w][0];
@@ -1629,42 +1705,22 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   P.matrix_norm = L.orig_spectral_bound;
   P.offset = L.host ? L.host->objective_offset : 0.0;
   P.round_rho = anchored ? req.round_rho : 0.0;
-  *(volatile int32_t *)c->cancel_mapped = (req.cancel && *req.cancel) ? 1 : 0;
   a.cancel = c->cancel_mapped_dev;
   PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
-  const double setup_ms = ms_since(t_start);
-  P.setup_ms = setup_ms;
+  j.setup_ms = ms_since(j.t0);
+  P.setup_ms = j.setup_ms;
+  return PRIMA_OK;
+}
 
-  cudaEvent_t e0, e1;
-  PRIMA_CUDA_TRY(cudaEventCreate(&e0));
-  PRIMA_CUDA_TRY(cudaEventCreate(&e1));
-  void *kargs[] = {(void *)&a};
-  PRIMA_CUDA_TRY(cudaEventRecord(e0, s));
-  cudaError_t le = cudaLaunchCooperativeKernel((const void *)dev::pdhg_kernel<T>, dim3(blocks), dim3(dev::kThreads),
-                                               kargs, dyn_smem<T>(), s);
-  if (le != cudaSuccess) {
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    set_error(std::string("cooperative launch: ") + cudaGetErrorString(le));
-    return PRIMA_ERR_CUDA;
-  }
-  PRIMA_CUDA_TRY(cudaEventRecord(e1, s));
-  // Wait; meanwhile forward the caller's cancel flag to the mapped flag the
-  // device polls at evaluation points.
-  for (int spin = 0;; spin++) {
-    const cudaError_t q = cudaEventQuery(e1);
-    if (q == cudaSuccess) break;
-    if (q != cudaErrorNotReady) {
-      set_error(std::string("solver kernel: ") + cudaGetErrorString(q));
-      return PRIMA_ERR_CUDA;
-    }
-    if (req.cancel && *req.cancel) *(volatile int32_t *)c->cancel_mapped = 1;
-    if (spin > 200) std::this_thread::sleep_for(std::chrono::microseconds(20));
-  }
-  float kms = 0.f;
-  cudaEventElapsedTime(&kms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+// After the launch: the final Control record, the solution in caller units
+// and the info fields.  kms: the launch's device time.
+template <typename T>
+int32_t finish_job(Ctx *c, Job<T> &j, float kms, int blocks) {
+  const SolveRequest &req = j.req;
+  const dev::Args<T> &a = j.a;
+  const int32_t n = j.L->n, m = j.L->m;
+  dev::Control ctl;
+  dev::Sync sync;
   PRIMA_CUDA_TRY(cudaMemcpy(&ctl, a.ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
   PRIMA_CUDA_TRY(cudaMemcpy(&sync, a.sync, sizeof(sync), cudaMemcpyDeviceToHost));
   if (sync.abort) ctl.error = PRIMA_ERR_TIMEOUT;
@@ -1684,9 +1740,9 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   info->final_step_size = ctl.step;
   info->final_primal_weight = ctl.weight;
   info->device_ms = kms;
-  info->setup_ms = setup_ms;
+  info->setup_ms = j.setup_ms;
   info->trials = ctl.total_trials;
-  info->solve_ms = (int64_t)ms_since(t_start);
+  info->solve_ms = (int64_t)ms_since(j.t0);
   if (req.rounds) *req.rounds = ctl.rounds;
   if (std::getenv("PRIMA_PHASE_TIMES")) {
     dev::Prof prof;
@@ -1706,6 +1762,175 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
     return PRIMA_ERR_TIMEOUT;
   }
   return PRIMA_OK;
+}
+
+// Waits for the event ending a launch, forwarding the caller's cancel flag
+// to the mapped flag the device polls at evaluation points.
+int32_t wait_forwarding_cancel(Ctx *c, cudaEvent_t done, const volatile int32_t *cancel) {
+  for (int spin = 0;; spin++) {
+    const cudaError_t q = cudaEventQuery(done);
+    if (q == cudaSuccess) return PRIMA_OK;
+    if (q != cudaErrorNotReady) {
+      set_error(std::string("solver kernel: ") + cudaGetErrorString(q));
+      return PRIMA_ERR_CUDA;
+    }
+    if (cancel && *cancel) *(volatile int32_t *)c->cancel_mapped = 1;
+    if (spin > 200) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+}
+
+// One cooperative launch of `kernel` with the given arguments, timed by CUDA
+// events on the context stream.
+template <typename T>
+int32_t launch_timed(Ctx *c, const void *kernel, int blocks, void **kargs, const volatile int32_t *cancel,
+                     float *kms) {
+  cudaStream_t s = c->stream;
+  cudaEvent_t e0, e1;
+  PRIMA_CUDA_TRY(cudaEventCreate(&e0));
+  PRIMA_CUDA_TRY(cudaEventCreate(&e1));
+  int32_t rc = PRIMA_OK;
+  cudaEventRecord(e0, s);
+  const cudaError_t le =
+      cudaLaunchCooperativeKernel(kernel, dim3(blocks), dim3(dev::kThreads), kargs, dyn_smem<T>(), s);
+  if (le != cudaSuccess) {
+    set_error(std::string("cooperative launch: ") + cudaGetErrorString(le));
+    rc = PRIMA_ERR_CUDA;
+  } else {
+    cudaEventRecord(e1, s);
+    rc = wait_forwarding_cancel(c, e1, cancel);
+    if (!rc) cudaEventElapsedTime(kms, e0, e1);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+// Pdhg.Solve on a prepared problem: the host prologue, then the whole
+// iteration in one cooperative launch.
+template <typename T>
+int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::time_point t_start) {
+  Job<T> j;
+  j.L = &L;
+  j.req = req;
+  j.t0 = t_start;
+  int32_t rc;
+  if ((rc = prepare_job(c, j))) return rc;
+  int max_blocks = 0;
+  if ((rc = max_coresident_blocks<T>(c, &max_blocks))) return rc;
+  const int blocks = team_blocks(L.n, L.m, max_blocks);
+  const StateLayout<T> S(L.n, L.m, blocks, req.anchored);
+  if ((rc = c->solver_arena.reserve(S.bytes))) return rc;
+  *(volatile int32_t *)c->cancel_mapped = (req.cancel && *req.cancel) ? 1 : 0;
+  if ((rc = setup_job(c, j, (char *)c->solver_arena.ptr, S, blocks))) return rc;
+  void *kargs[] = {(void *)&j.a};
+  float kms = 0.f;
+  if ((rc = launch_timed<T>(c, (const void *)dev::pdhg_kernel<T>, blocks, kargs, req.cancel, &kms))) return rc;
+  return finish_job(c, j, kms, blocks);
+}
+
+template <typename T>
+int32_t max_coresident_batch_blocks(Ctx *c, int *out) {
+  int per_sm = 0;
+  PRIMA_CUDA_TRY(cudaFuncSetAttribute(dev::pdhg_batch_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)dyn_smem<T>()));
+  PRIMA_CUDA_TRY(
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::pdhg_batch_kernel<T>, dev::kThreads, dyn_smem<T>()));
+  if (per_sm < 1) {
+    set_error("batch solver kernel cannot be resident on an SM");
+    return PRIMA_ERR_CUDA;
+  }
+  *out = per_sm * c->num_sms;
+  return PRIMA_OK;
+}
+
+// Team size for a batch: a power of two, about twice the share of the
+// co-resident blocks that the largest instance's work represents (so the
+// largest instance, started first, is not the one that finishes last), and
+// never more blocks than the largest instance would use alone.
+inline int batch_team_blocks(const std::vector<int> &solo, int max_blocks) {
+  int64_t total = 0;
+  int largest = 1;
+  for (int b : solo) {
+    total += b;
+    largest = std::max(largest, b);
+  }
+  const double target = 2.0 * (double)max_blocks * (double)largest / (double)std::max<int64_t>(total, 1);
+  int tb = 1;
+  while (tb * 2 <= target && tb * 2 <= largest && tb * 2 <= max_blocks) tb *= 2;
+  return tb;
+}
+
+// Many solves in one cooperative launch of pdhg_batch_kernel (see there).
+// Every job is prepared and set up as a single solve would be, with its own
+// state in the batch arena; the Args records go to the device in order of
+// decreasing size, the order in which the teams take them.
+template <typename T>
+int32_t solve_batch_on_device(Ctx *c, std::vector<Job<T>> &jobs, const volatile int32_t *cancel) {
+  const int count = (int)jobs.size();
+  if (count == 0) return PRIMA_OK;
+  int32_t rc;
+  for (auto &j : jobs)
+    if ((rc = prepare_job(c, j))) return rc;
+  int max_blocks = 0;
+  if ((rc = max_coresident_batch_blocks<T>(c, &max_blocks))) return rc;
+  std::vector<int> solo((size_t)count);
+  std::vector<int64_t> size((size_t)count);
+  for (int i = 0; i < count; i++) {
+    const PreparedLp &L = *jobs[i].L;
+    solo[i] = team_blocks(L.n, L.m, max_blocks);
+    size[i] = (int64_t)L.n + L.m + L.nnz;
+  }
+  const int tb = batch_team_blocks(solo, max_blocks);
+  const int teams = std::min(count, max_blocks / tb);
+  std::vector<int> order((size_t)count);
+  for (int i = 0; i < count; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return size[x] > size[y]; });
+
+  std::vector<StateLayout<T>> layouts;
+  std::vector<size_t> offs;
+  layouts.reserve((size_t)count);
+  size_t total = 0;
+  for (int i = 0; i < count; i++) {
+    layouts.emplace_back(jobs[i].L->n, jobs[i].L->m, tb, jobs[i].req.anchored);
+    offs.push_back(total);
+    total += (layouts.back().bytes + 255) & ~(size_t)255;
+  }
+  const size_t off_args = total;
+  total += ((size_t)count * sizeof(dev::Args<T>) + 255) & ~(size_t)255;
+  const size_t off_queue = total;
+  total += ((size_t)(teams + 1) * 4 + 255) & ~(size_t)255;
+  if ((rc = c->batch_arena.reserve(total))) return rc;
+  char *base = (char *)c->batch_arena.ptr;
+  *(volatile int32_t *)c->cancel_mapped = (cancel && *cancel) ? 1 : 0;
+  for (int i = 0; i < count; i++)
+    if ((rc = setup_job(c, jobs[i], base + offs[i], layouts[i], tb))) return rc;
+
+  std::vector<dev::Args<T>> args((size_t)count);
+  for (int i = 0; i < count; i++) args[i] = jobs[order[i]].a;
+  std::vector<int32_t> queue((size_t)teams + 1, 0);
+  queue[0] = teams;  // team k starts with instance k; the queue hands out the rest
+  PRIMA_CUDA_TRY(cudaMemcpyAsync(base + off_args, args.data(), (size_t)count * sizeof(dev::Args<T>),
+                                 cudaMemcpyHostToDevice, c->stream));
+  PRIMA_CUDA_TRY(cudaMemcpyAsync(base + off_queue, queue.data(), queue.size() * 4, cudaMemcpyHostToDevice, c->stream));
+  const dev::Args<T> *d_args = (const dev::Args<T> *)(base + off_args);
+  int32_t *d_queue = (int32_t *)(base + off_queue);
+  int32_t *d_team_next = d_queue + 1;
+  int cnt = count, tbv = tb;
+  void *kargs[] = {(void *)&d_args, (void *)&cnt, (void *)&tbv, (void *)&d_queue, (void *)&d_team_next};
+  float kms = 0.f;
+  if ((rc = launch_timed<T>(c, (const void *)dev::pdhg_batch_kernel<T>, teams * tb, kargs, cancel, &kms))) return rc;
+  int32_t first_error = PRIMA_OK;
+  for (int i = 0; i < count; i++) {
+    dev::Control ctl;
+    PRIMA_CUDA_TRY(cudaMemcpy(&ctl, jobs[i].a.ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+    rc = finish_job(c, jobs[i], kms, tb);
+    // this instance's own device time, from the timer readings it took
+    if (ctl.t_end > ctl.t0 && ctl.t0) jobs[i].req.info->device_ms = 1e-6 * (double)(ctl.t_end - ctl.t0);
+    if (rc && !first_error) first_error = rc;
+  }
+  if (std::getenv("PRIMA_PHASE_TIMES"))
+    std::fprintf(stderr, "[prima batch] %d instances, %d teams x %d blocks, %.2f ms\n", count, teams, tb, kms);
+  return first_error;
 }
 
 // Equilibrate (again) if the prepared problem was scaled differently.
@@ -1834,6 +2059,109 @@ int32_t mixed_dispatch(Ctx *c, PreparedLp &L, const prima_lp *lp, const prima_pa
     return PRIMA_OK;
   }
   return mixed_passes(c, L, lp, params, mixed, cancel, x_out, y_out, rc_out, info, minfo, t0);
+}
+
+// mixed_passes for many instances: each pass runs for every instance that
+// needs it in one batch launch.  Per instance the decisions are exactly
+// mixed_passes' (certificate re-check, refinement only after an Optimal
+// reduced pass, otherwise the FP64 finish).
+int32_t mixed_passes_batch(Ctx *c, std::vector<std::unique_ptr<PreparedLp>> &Ls, const prima_lp *lps,
+                           const prima_params *p, const prima_mixed_params *mp, const volatile int32_t *cancel,
+                           double *const *x_out, double *const *y_out, double *const *rc_out,
+                           prima_solution_info *infos, prima_mixed_info *minfos, Clock::time_point t0) {
+  const int32_t count = (int32_t)Ls.size();
+  prima_params rp = *p;
+  rp.eps_abs = std::max(p->eps_abs, mp->reduced_tolerance);
+  rp.eps_rel = std::max(p->eps_rel, mp->reduced_tolerance);
+  rp.max_iterations = std::min(p->max_iterations, mp->reduced_max_iterations);
+  if (p->time_limit_ms >= 0) rp.time_limit_ms = std::max(1.0, std::floor(p->time_limit_ms * mp->reduced_time_share));
+  rp.infeasibility_tolerance = std::max(p->infeasibility_tolerance, mp->reduced_tolerance);
+  std::vector<std::vector<double>> rx((size_t)count), ry((size_t)count), rrc((size_t)count);
+  std::vector<prima_solution_info> rinfo((size_t)count);
+  int32_t rc;
+  {
+    std::vector<Job<float>> jobs((size_t)count);
+    for (int32_t i = 0; i < count; i++) {
+      rx[i].resize((size_t)Ls[i]->n);
+      ry[i].resize((size_t)Ls[i]->m);
+      rrc[i].resize((size_t)Ls[i]->n);
+      jobs[i].L = Ls[i].get();
+      jobs[i].req = SolveRequest{&rp, nullptr, cancel, rx[i].data(), ry[i].data(), rrc[i].data(), &rinfo[i]};
+      jobs[i].t0 = t0;
+    }
+    if ((rc = solve_batch_on_device(c, jobs, cancel))) return rc;
+  }
+  prima_params fp = *p;
+  const auto t1 = Clock::now();
+  std::vector<prima_warm_start> ws((size_t)count);
+  std::vector<Job<float>> anchored;
+  std::vector<Job<double>> fp64;
+  std::vector<int32_t> who32, who64;
+  for (int32_t i = 0; i < count; i++) {
+    const prima_lp *lp = &lps[i];
+    const int st = rinfo[i].status;
+    const bool conclusive = st == PRIMA_STATUS_OPTIMAL || st == PRIMA_STATUS_PRIMAL_INFEASIBLE ||
+                            st == PRIMA_STATUS_DUAL_INFEASIBLE;
+    const bool cert_holds = conclusive && st != PRIMA_STATUS_OPTIMAL &&
+                            classify_fp64(lp, rx[i].data(), ry[i].data(), p->infeasibility_tolerance) == st;
+    prima_mixed_info &mi = minfos[i];
+    std::memset(&mi, 0, sizeof(mi));
+    mi.reduced_iterations = rinfo[i].iterations;
+    mi.reduced_restarts = rinfo[i].restarts;
+    mi.reduced_ms = rinfo[i].solve_ms;
+    double *xo = x_out ? x_out[i] : nullptr, *yo = y_out ? y_out[i] : nullptr, *rco = rc_out ? rc_out[i] : nullptr;
+    if (!mp->always_refine && cert_holds) {
+      infos[i] = rinfo[i];
+      if (xo) std::memcpy(xo, rx[i].data(), (size_t)lp->num_variables * 8);
+      if (yo) std::memcpy(yo, ry[i].data(), (size_t)lp->num_constraints * 8);
+      if (rco) std::memcpy(rco, rrc[i].data(), (size_t)lp->num_variables * 8);
+      continue;
+    }
+    bool usable = true;
+    for (double v : rx[i]) usable = usable && std::isfinite(v);
+    for (double v : ry[i]) usable = usable && std::isfinite(v);
+    prima_warm_start &w = ws[i];
+    w.primal = rx[i].data();
+    w.dual = ry[i].data();
+    w.step_size = (std::isfinite(rinfo[i].final_step_size) && rinfo[i].final_step_size > 0.0) ? rinfo[i].final_step_size
+                                                                                             : NAN;
+    w.primal_weight = (std::isfinite(rinfo[i].final_primal_weight) && rinfo[i].final_primal_weight > 0.0)
+                          ? rinfo[i].final_primal_weight
+                          : NAN;
+    SolveRequest finish{&fp, usable ? &w : nullptr, cancel, xo, yo, rco, &infos[i]};
+    if (mp->scheme == PRIMA_MIXED_REFINEMENT && st == PRIMA_STATUS_OPTIMAL) {
+      finish.anchored = true;
+      finish.round_rho = mp->round_reduction > 0.0 ? 1.0 / mp->round_reduction : 0.0;
+      finish.rounds = &mi.refinement_rounds;
+      Job<float> j;
+      j.L = Ls[i].get();
+      j.req = finish;
+      j.t0 = t1;
+      anchored.push_back(j);
+      who32.push_back(i);
+    } else {
+      Job<double> j;
+      j.L = Ls[i].get();
+      j.req = finish;
+      j.t0 = t1;
+      fp64.push_back(j);
+      who64.push_back(i);
+    }
+  }
+  if ((rc = solve_batch_on_device(c, anchored, cancel))) return rc;
+  if ((rc = solve_batch_on_device(c, fp64, cancel))) return rc;
+  auto close = [&](int32_t i) {
+    prima_mixed_info &mi = minfos[i];
+    mi.refinement_iterations = infos[i].iterations;
+    mi.refinement_ms = infos[i].solve_ms;
+    mi.refined = 1;
+    infos[i].device_ms += rinfo[i].device_ms;
+    infos[i].trials += rinfo[i].trials;
+    infos[i].solve_ms = (int64_t)ms_since(t0);
+  };
+  for (int32_t i : who32) close(i);
+  for (int32_t i : who64) close(i);
+  return PRIMA_OK;
 }
 
 // CUDA events on the context stream bracketing a whole coarse call.
@@ -1977,6 +2305,69 @@ extern "C" int32_t prima_pdhg_solve_batch(prima_handle ctx, int32_t count, const
                                           double *const *x_out, double *const *y_out, double *const *rc_out,
                                           prima_solution_info *infos) {
   CTX_OR_RETURN(ctx);
-  set_error("prima_pdhg_solve_batch: not built yet");
-  return PRIMA_ERR_INVALID_ARGUMENT;
+  const auto t0 = Clock::now();
+  int32_t rc;
+  if (count < 0 || (count > 0 && (!lps || !infos)))
+    return (set_error("requirement failed: count must be non-negative and lps, infos non-NULL"),
+            PRIMA_ERR_INVALID_ARGUMENT);
+  if ((rc = validate_params(params))) return rc;
+  for (int32_t i = 0; i < count; i++)
+    if ((rc = validate_lp(&lps[i]))) return rc;
+  Span span(c->stream);
+  std::vector<std::unique_ptr<PreparedLp>> prepared((size_t)count);
+  for (int32_t i = 0; i < count; i++) {
+    prepared[i] = std::make_unique<PreparedLp>();
+    if ((rc = ensure_prepared(c, *prepared[i], &lps[i], params))) return rc;
+  }
+  auto request = [&](int32_t i) {
+    return SolveRequest{params, nullptr, cancel, x_out ? x_out[i] : nullptr, y_out ? y_out[i] : nullptr,
+                        rc_out ? rc_out[i] : nullptr, &infos[i]};
+  };
+  if (c->bits == 64) {
+    std::vector<Job<double>> jobs((size_t)count);
+    for (int32_t i = 0; i < count; i++) jobs[i].L = prepared[i].get(), jobs[i].req = request(i), jobs[i].t0 = t0;
+    rc = solve_batch_on_device(c, jobs, cancel);
+  } else {
+    std::vector<Job<float>> jobs((size_t)count);
+    for (int32_t i = 0; i < count; i++) jobs[i].L = prepared[i].get(), jobs[i].req = request(i), jobs[i].t0 = t0;
+    rc = solve_batch_on_device(c, jobs, cancel);
+  }
+  const double span_ms = span.stop();
+  for (int32_t i = 0; i < count; i++) infos[i].span_ms = span_ms;
+  return rc;
+}
+
+extern "C" int32_t prima_mixed_solve_batch(prima_handle ctx, int32_t count, const prima_lp *lps,
+                                           const prima_params *params, const prima_mixed_params *mixed,
+                                           const volatile int32_t *cancel, double *const *x_out,
+                                           double *const *y_out, double *const *rc_out, prima_solution_info *infos,
+                                           prima_mixed_info *minfos) {
+  CTX_OR_RETURN(ctx);
+  const auto t0 = Clock::now();
+  int32_t rc;
+  if (count < 0 || (count > 0 && (!lps || !infos || !minfos)))
+    return (set_error("requirement failed: count must be non-negative and lps, infos, mixed_infos non-NULL"),
+            PRIMA_ERR_INVALID_ARGUMENT);
+  if ((rc = validate_mixed(mixed)) || (rc = validate_params(params))) return rc;
+  for (int32_t i = 0; i < count; i++)
+    if ((rc = validate_lp(&lps[i]))) return rc;
+  if (c->bits == 64) {  // a float64 device skips the reduced pass (MixedPrecision.scala:111-113)
+    rc = prima_pdhg_solve_batch(ctx, count, lps, params, cancel, x_out, y_out, rc_out, infos);
+    for (int32_t i = 0; i < count && !rc; i++) {
+      std::memset(&minfos[i], 0, sizeof(minfos[i]));
+      minfos[i].refinement_iterations = infos[i].iterations;
+      minfos[i].refinement_ms = infos[i].solve_ms;
+    }
+    return rc;
+  }
+  Span span(c->stream);
+  std::vector<std::unique_ptr<PreparedLp>> prepared((size_t)count);
+  for (int32_t i = 0; i < count; i++) {
+    prepared[i] = std::make_unique<PreparedLp>();
+    if ((rc = ensure_prepared(c, *prepared[i], &lps[i], params))) return rc;
+  }
+  rc = mixed_passes_batch(c, prepared, lps, params, mixed, cancel, x_out, y_out, rc_out, infos, minfos, t0);
+  const double span_ms = span.stop();
+  for (int32_t i = 0; i < count; i++) infos[i].span_ms = span_ms;
+  return rc;
 }

@@ -107,6 +107,7 @@ struct Control {
   double inv_w, tau, sigma, error_at_restart;
   double last_candidate, round_err;
   int32_t rounds, pad3;
+  uint64_t t_end;  // global timer when the solve finished (with t0: its device time)
   Kkt current, average, final_kkt;
 };
 
@@ -146,7 +147,7 @@ struct Args {
   double *xo, *yo, *rco;
   double *partials;  // [kMaxQ][max_blocks]
   int32_t max_blocks, anchored;
-  const int2 *tiles_k, *tiles_t;  // warp-tile tables of K and K': (first row, first nonzero), + a sentinel
+  const int2 *tiles_k, *tiles_t;  // tile tables of K and K': (first row, first nonzero), + a sentinel
   int32_t ntiles_k, ntiles_t;
   Prof *prof;
   // Anchored (refinement) mode: the iterate is a correction (x^, y^) to an
@@ -161,6 +162,11 @@ struct Args {
   Control *ctl;
   Sync *sync;
   const volatile int32_t *cancel;
+  // batch launches: the shared queue of instance indices, and per team the
+  // index its deciding block took when this instance finished.  nullptr for
+  // a single solve.
+  int32_t *queue, *team_next;
+  int32_t team, pad2;
   Params P;
 };
 

@@ -118,6 +118,9 @@ SIGNATURES = {
                                       _DP, _DP, _DP, C.POINTER(CInfo), C.POINTER(CMixedInfo)]),
     "prima_pdhg_solve_batch": (C.c_int32, [_H, C.c_int32, C.POINTER(CLp), C.POINTER(CParams), _IP,
                                            C.POINTER(_DP), C.POINTER(_DP), C.POINTER(_DP), C.POINTER(CInfo)]),
+    "prima_mixed_solve_batch": (C.c_int32, [_H, C.c_int32, C.POINTER(CLp), C.POINTER(CParams),
+                                            C.POINTER(CMixedParams), _IP, C.POINTER(_DP), C.POINTER(_DP),
+                                            C.POINTER(_DP), C.POINTER(CInfo), C.POINTER(CMixedInfo)]),
     "prima_problem_create": (C.c_int32, [_H, C.POINTER(CLp), C.POINTER(CParams), _HP]),
     "prima_problem_free": (C.c_int32, [_H, _H]),
     "prima_problem_solve": (C.c_int32, [_H, _H, C.POINTER(CParams), C.POINTER(CWarm), _IP, _DP, _DP, _DP,
@@ -395,6 +398,38 @@ def mixed_solve(problem: LpProblem, params: PdhgParams = PdhgParams(),
                                int(minfo.reduced_ms), minfo.refinement_iterations, int(minfo.refinement_ms),
                                bool(minfo.refined), minfo.refinement_rounds)
     return res
+
+
+def mixed_solve_batch(problems: Sequence[LpProblem], params: PdhgParams = PdhgParams(),
+                      mixed: MixedPrecisionParams = MixedPrecisionParams(), scheme: int = None,
+                      round_reduction: float = 0.0, cancel: Optional[C.c_int32] = None, device: int = 0,
+                      ctx: Optional[Context] = None) -> list[MixedPrecisionResult]:
+    """``mixed_solve`` for many independent LPs, each pass one device launch
+    for all of them."""
+    scheme = DEFAULT_SCHEME if scheme is None else scheme
+    ctx = ctx or context(device, 32)
+    k = len(problems)
+    views = [_LpView(p) for p in problems]
+    arr = (CLp * k)(*[v.c for v in views])
+    xs = [np.zeros(p.num_variables) for p in problems]
+    ys = [np.zeros(p.num_constraints) for p in problems]
+    rcs = [np.zeros(p.num_variables) for p in problems]
+    px = (_DP * k)(*[_dp(a) for a in xs])
+    py = (_DP * k)(*[_dp(a) for a in ys])
+    prc = (_DP * k)(*[_dp(a) for a in rcs])
+    infos, minfos = (CInfo * k)(), (CMixedInfo * k)()
+    cp = to_c_params(params)
+    mp = to_c_mixed(mixed, scheme, round_reduction)
+    _check(ctx.lib.prima_mixed_solve_batch(ctx.handle, k, arr, C.byref(cp), C.byref(mp),
+                                           None if cancel is None else C.cast(C.byref(cancel), _IP), px, py, prc,
+                                           infos, minfos))
+    out = []
+    for i in range(k):
+        mi = minfos[i]
+        out.append(MixedPrecisionResult(_solution(infos[i], xs[i], ys[i], rcs[i]), mi.reduced_iterations,
+                                        mi.reduced_restarts, int(mi.reduced_ms), mi.refinement_iterations,
+                                        int(mi.refinement_ms), bool(mi.refined), mi.refinement_rounds))
+    return out
 
 
 class DeviceProblem:
