@@ -1843,21 +1843,28 @@ int32_t max_coresident_batch_blocks(Ctx *c, int *out) {
   return PRIMA_OK;
 }
 
-// Team size for a batch: a power of two, about twice the share of the
-// co-resident blocks that the largest instance's work represents (so the
-// largest instance, started first, is not the one that finishes last), and
-// never more blocks than the largest instance would use alone.
-inline int batch_team_blocks(const std::vector<int> &solo, int max_blocks) {
-  int64_t total = 0;
-  int largest = 1;
-  for (int b : solo) {
-    total += b;
-    largest = std::max(largest, b);
+// Team size for a batch: the power of two that minimises a simple model of
+// the makespan per iteration round.  An iteration of an instance with w tiles
+// (K and K' together) on tb blocks costs about c0 + c1 w / tb: c0 for the two
+// team barriers, c1 for a block to stream one tile.  With `teams` teams the
+// round takes at least the slowest instance's iteration and at least the
+// total spread over the teams.
+inline int batch_team_blocks(const std::vector<int64_t> &tiles, int max_blocks) {
+  constexpr double c0 = 20.0, c1 = 2.0;  // microseconds, measured on config-2-sized teams
+  int best = 1;
+  double best_cost = std::numeric_limits<double>::infinity();
+  for (int tb = 1; tb <= max_blocks; tb *= 2) {
+    const int teams = std::min<int64_t>((int64_t)tiles.size(), max_blocks / tb);
+    double slowest = 0.0, sum = 0.0;
+    for (int64_t w : tiles) {
+      const double t = c0 + c1 * (double)w / tb;
+      slowest = std::max(slowest, t);
+      sum += t;
+    }
+    const double cost = std::max(slowest, sum / std::max(teams, 1));
+    if (cost < best_cost) best_cost = cost, best = tb;
   }
-  const double target = 2.0 * (double)max_blocks * (double)largest / (double)std::max<int64_t>(total, 1);
-  int tb = 1;
-  while (tb * 2 <= target && tb * 2 <= largest && tb * 2 <= max_blocks) tb *= 2;
-  return tb;
+  return best;
 }
 
 // Many solves in one cooperative launch of pdhg_batch_kernel (see there).
@@ -1873,14 +1880,14 @@ int32_t solve_batch_on_device(Ctx *c, std::vector<Job<T>> &jobs, const volatile 
     if ((rc = prepare_job(c, j))) return rc;
   int max_blocks = 0;
   if ((rc = max_coresident_batch_blocks<T>(c, &max_blocks))) return rc;
-  std::vector<int> solo((size_t)count);
-  std::vector<int64_t> size((size_t)count);
+  std::vector<int64_t> tiles((size_t)count), size((size_t)count);
+  const int w = sizeof(T) == 8;
   for (int i = 0; i < count; i++) {
     const PreparedLp &L = *jobs[i].L;
-    solo[i] = team_blocks(L.n, L.m, max_blocks);
+    tiles[i] = (int64_t)L.ntiles[w][0] + L.ntiles[w][1];
     size[i] = (int64_t)L.n + L.m + L.nnz;
   }
-  const int tb = batch_team_blocks(solo, max_blocks);
+  const int tb = batch_team_blocks(tiles, max_blocks);
   const int teams = std::min(count, max_blocks / tb);
   std::vector<int> order((size_t)count);
   for (int i = 0; i < count; i++) order[i] = i;
