@@ -166,6 +166,45 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+BATCH_EPS = 1e-6
+
+
+def run_batch(args, rank, world, dist, barrier):
+    """Config 3: an uneven sweep of ``--batch`` DC-LOPF instances (buses
+    U{100..2000}, snapshots U{24..168}, load scale U[0.6, 0.95], seeded), FP32
+    refinement to 1e-6, each pass one launch for all of this rank's
+    instances.  Ranks take longest-processing-time shards; LPs/s is all
+    instances over the slowest rank's time."""
+    import torch
+    from noaidi_b200.prima import MixedPrecisionParams, PdhgParams, cuda, generators as G
+    from noaidi_b200.prima.sharding import instance_size, shard
+    problems = G.lopf_batch(seed=0, count=args.batch)
+    mine = shard([instance_size(p) for p in problems], world)[rank]
+    params = PdhgParams(eps_abs=BATCH_EPS, eps_rel=BATCH_EPS, max_iterations=args.max_iterations)
+    mixed = MixedPrecisionParams(reduced_max_iterations=args.max_iterations)
+    ctx = cuda.Context(int(os.environ.get("LOCAL_RANK", "0")), 32)
+    barrier()
+    t = time.perf_counter()
+    res = cuda.mixed_solve_batch([problems[i] for i in mine], params, mixed, scheme=cuda.MIXED_REFINEMENT,
+                                 round_reduction=args.round_reduction, ctx=ctx) if mine else []
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t
+    span = max((r.solution.span_ms for r in res), default=0.0) / 1e3
+    agg = torch.tensor([span, secs], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(agg, op=dist.ReduceOp.MAX)
+    ctx.close()
+    its = [r.reduced_iterations + r.refinement_iterations for r in res]
+    statuses = sorted({r.solution.status.name for r in res})
+    return {"workload": f"config 3: {args.batch} uneven DC-LOPF instances, FP32 refinement to {BATCH_EPS:g}",
+            "instances": args.batch, "lps_per_s": args.batch / float(agg[0]), "seconds": float(agg[0]),
+            "wall_seconds": float(agg[1]), "statuses_rank0": statuses,
+            "iterations_rank0": {"min": int(min(its)), "median": float(np.median(its)), "max": int(max(its))}
+            if its else None,
+            "columns": int(sum(p.num_variables for p in problems)),
+            "nnz": int(sum(p.constraint_matrix.nnz for p in problems))}
+
+
 def run_profile_case(args) -> None:
     """A bounded run for profilers: the workload (optionally fewer snapshots)
     resident on the device, one plain PDHG solve capped at
@@ -194,6 +233,9 @@ def main():
     ap.add_argument("--full-fp64", action="store_true", help="solve FP64 to tolerance instead of sampling")
     ap.add_argument("--cpu-sample-iterations", type=int, default=128)
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="also solve this many config-3 instances (uneven LOPF sweep) to 1e-6 as batches "
+                         "and report LPs/s under 'batch' (0: off)")
     ap.add_argument("--profile-iterations", type=int, default=0,
                     help="only run this many PDHG iterations of the workload (a bounded case for ncu) and exit")
     ap.add_argument("--profile-precision", type=int, default=32, choices=[32, 64])
@@ -265,6 +307,8 @@ def main():
     fp64 = res64.solve(p64, want_solution=False)
     fp64_ms_per_iter = fp64.device_ms / max(1, fp64.iterations)
 
+    batch_line = run_batch(args, rank, world, dist, barrier) if args.batch else None
+
     if rank == 0:
         pk, pk_src = peaks()
         n, m, nnz = problem.num_variables, problem.num_constraints, problem.constraint_matrix.nnz
@@ -308,6 +352,8 @@ def main():
                             "traffic": TRAFFIC_BYTES_PER_TRIAL * trials32 / len(results) if TRAFFIC_BYTES_PER_TRIAL else None,
                             "peak_source": pk_src,
                             "per_trial_bytes": byts / max(1, trials32), "kernel_ms": 1e3 * kern_s / steps}
+        if batch_line:
+            line["batch"] = batch_line
         if not args.skip_cpu:
             per_iter, done = cpu_sample(problem, args.cpu_sample_iterations)
             lps = 1.0 / (per_iter * iters64)
