@@ -261,6 +261,12 @@ int32_t prima_mixed_solve_batch(prima_handle ctx, int32_t count, const prima_lp 
 int32_t prima_problem_create(prima_handle ctx, const prima_lp *lp, const prima_params *params,
                              prima_handle *problem);
 int32_t prima_problem_free(prima_handle ctx, prima_handle problem);
+/* Replaces the resident problem's variable bounds (n each; lower <= upper,
+ * infinities allowed), keeping its upload and equilibration: a
+ * branch-and-bound node is its parent's LP with one bound moved
+ * (BranchAndBound.scala:264-276, the node's LpProblem with new
+ * variableLower/variableUpper). */
+int32_t prima_problem_set_bounds(prima_handle ctx, prima_handle problem, const double *lower, const double *upper);
 /* As prima_pdhg_solve / prima_mixed_solve on a resident problem. */
 int32_t prima_problem_solve(prima_handle ctx, prima_handle problem, const prima_params *params,
                             const prima_warm_start *warm_start, const volatile int32_t *cancel,

@@ -113,6 +113,9 @@ struct PreparedLp {
   int32_t prepare(const prima_lp *lp, const prima_params *p, cudaStream_t s);
   template <typename T>
   int32_t materialise(cudaStream_t s);
+  // New variable bounds for the prepared problem: the scaling depends on the
+  // matrix alone, so only the bounds' scaled and storage-type copies change.
+  int32_t set_bounds(const double *lower, const double *upper, cudaStream_t s);
 };
 
 // Owned host copy of a problem (for problem handles).

@@ -120,6 +120,16 @@ __global__ void k_scaled_vectors(int32_t n, int32_t m, const double *__restrict_
   for (int32_t r = i0; r < m; r += st) sq[r] = q[r] * rs[r];
 }
 
+// the bounds' part of k_scaled_vectors
+__global__ void k_scaled_bounds(int32_t n, const double *__restrict__ l, const double *__restrict__ u,
+                                const double *__restrict__ cs, double *__restrict__ sl, double *__restrict__ su) {
+  for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const double d = cs[j];
+    sl[j] = l[j] / d;
+    su[j] = u[j] / d;
+  }
+}
+
 template <typename T>
 __global__ void k_gather_cast(int64_t nnz, const int32_t *__restrict__ perm, const double *__restrict__ v,
                               T *__restrict__ out) {
@@ -309,6 +319,26 @@ int32_t PreparedLp::materialise(cudaStream_t s) {
   if (m) k_cast<T><<<blocks_for(m), kT, 0, s>>>(m, sq(), (T *)pcpy.q.ptr);
   PRIMA_CUDA_TRY(cudaGetLastError());
   precision_ready[w] = true;
+  return PRIMA_OK;
+}
+
+int32_t PreparedLp::set_bounds(const double *lower, const double *upper, cudaStream_t s) {
+  if (n == 0) return PRIMA_OK;
+  PRIMA_CUDA_TRY(cudaMemcpyAsync(b_l0.ptr, lower, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+  PRIMA_CUDA_TRY(cudaMemcpyAsync(b_u0.ptr, upper, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+  k_scaled_bounds<<<blocks_for(n), kT, 0, s>>>(n, l0(), u0(), cs(), sl_(), su_());
+  if (precision_ready[0]) {
+    k_cast<float><<<blocks_for(n), kT, 0, s>>>(n, sl(), (float *)copies[0].l.ptr);
+    k_cast<float><<<blocks_for(n), kT, 0, s>>>(n, su(), (float *)copies[0].u.ptr);
+  }
+  if (precision_ready[1]) {
+    k_cast<double><<<blocks_for(n), kT, 0, s>>>(n, sl(), (double *)copies[1].l.ptr);
+    k_cast<double><<<blocks_for(n), kT, 0, s>>>(n, su(), (double *)copies[1].u.ptr);
+  }
+  PRIMA_CUDA_TRY(cudaGetLastError());
+  PRIMA_CUDA_TRY(cudaMemcpyAsync(h_sl.data(), b_sl.ptr, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+  PRIMA_CUDA_TRY(cudaMemcpyAsync(h_su.data(), b_su.ptr, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+  PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
   return PRIMA_OK;
 }
 

@@ -2278,6 +2278,28 @@ extern "C" int32_t prima_problem_free(prima_handle ctx, prima_handle problem) {
   return PRIMA_OK;
 }
 
+extern "C" int32_t prima_problem_set_bounds(prima_handle ctx, prima_handle problem, const double *lower,
+                                            const double *upper) {
+  CTX_OR_RETURN(ctx);
+  auto it = c->problems.find(problem);
+  if (it == c->problems.end()) return (set_error("unknown problem handle"), PRIMA_ERR_CLOSED);
+  PreparedLp &L = *it->second;
+  const int32_t n = L.n;
+  if (n > 0 && (!lower || !upper)) return (set_error("requirement failed: bounds are NULL"), PRIMA_ERR_INVALID_ARGUMENT);
+  for (int32_t i = 0; i < n; i++)
+    if (!(lower[i] <= upper[i])) {
+      set_error("variable " + std::to_string(i) + " has empty bound interval [" + std::to_string(lower[i]) + ", " +
+                std::to_string(upper[i]) + "]");
+      return PRIMA_ERR_INVALID_ARGUMENT;
+    }
+  LpHostCopy &h = *L.owned;
+  h.lower.assign(lower, lower + n);
+  h.upper.assign(upper, upper + n);
+  h.lp.lower = h.lower.data();
+  h.lp.upper = h.upper.data();
+  return L.set_bounds(lower, upper, c->stream);
+}
+
 extern "C" int32_t prima_problem_solve(prima_handle ctx, prima_handle problem, const prima_params *params,
                                        const prima_warm_start *warm, const volatile int32_t *cancel, double *x_out,
                                        double *y_out, double *rc_out, prima_solution_info *info) {

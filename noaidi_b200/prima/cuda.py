@@ -123,6 +123,7 @@ SIGNATURES = {
                                             C.POINTER(_DP), C.POINTER(CInfo), C.POINTER(CMixedInfo)]),
     "prima_problem_create": (C.c_int32, [_H, C.POINTER(CLp), C.POINTER(CParams), _HP]),
     "prima_problem_free": (C.c_int32, [_H, _H]),
+    "prima_problem_set_bounds": (C.c_int32, [_H, _H, _DP, _DP]),
     "prima_problem_solve": (C.c_int32, [_H, _H, C.POINTER(CParams), C.POINTER(CWarm), _IP, _DP, _DP, _DP,
                                         C.POINTER(CInfo)]),
     "prima_problem_mixed_solve": (C.c_int32, [_H, _H, C.POINTER(CParams), C.POINTER(CMixedParams), _IP, _DP, _DP,
@@ -464,6 +465,19 @@ class DeviceProblem:
                                                 None if cancel is None else C.cast(C.byref(cancel), _IP), _dp(x),
                                                 _dp(y), _dp(rc), C.byref(info)))
         return _solution(info, x, y, rc)
+
+    def set_bounds(self, lower, upper) -> None:
+        """New variable bounds for the resident problem (``prima_problem_set_bounds``);
+        the upload and the equilibration are kept."""
+        lo = np.ascontiguousarray(lower, dtype=np.float64)
+        hi = np.ascontiguousarray(upper, dtype=np.float64)
+        n = self.problem.num_variables
+        if lo.shape != (n,) or hi.shape != (n,):
+            raise ValueError(f"requirement failed: bounds must have {n} entries")
+        _check(self.ctx.lib.prima_problem_set_bounds(self.ctx.handle, self.handle, _dp(lo), _dp(hi)))
+        p = self.problem
+        self.problem = LpProblem(p.objective, p.constraint_matrix, p.rhs, p.num_equalities, lo, hi,
+                                 p.objective_offset)
 
     def mixed_solve(self, params: PdhgParams = PdhgParams(), mixed: MixedPrecisionParams = MixedPrecisionParams(),
                     scheme: int = None, cancel: Optional[C.c_int32] = None, want_solution: bool = True,
