@@ -1849,15 +1849,18 @@ int32_t max_coresident_batch_blocks(Ctx *c, int *out) {
 // team barriers, c1 for a block to stream one tile.  With `teams` teams the
 // round takes at least the slowest instance's iteration and at least the
 // total spread over the teams.
-inline int batch_team_blocks(const std::vector<int64_t> &tiles, int max_blocks) {
+// No team is larger than the largest instance would use alone (a problem of
+// up to 4096 rows and columns runs as one block), so a batch of small LPs
+// solves each exactly as its own solve would.
+inline int batch_team_blocks(const std::vector<int64_t> &tiles, int max_blocks, int largest_solo) {
   constexpr double c0 = 20.0, c1 = 2.0;  // microseconds, measured on config-2-sized teams
   int best = 1;
   double best_cost = std::numeric_limits<double>::infinity();
-  for (int tb = 1; tb <= max_blocks; tb *= 2) {
+  for (int tb = 1; tb <= std::min(max_blocks, largest_solo); tb *= 2) {
     const int teams = std::min<int64_t>((int64_t)tiles.size(), max_blocks / tb);
     double slowest = 0.0, sum = 0.0;
     for (int64_t w : tiles) {
-      const double t = c0 + c1 * (double)w / tb;
+      const double t = c0 + c1 * (double)((w + tb - 1) / tb);
       slowest = std::max(slowest, t);
       sum += t;
     }
@@ -1882,12 +1885,14 @@ int32_t solve_batch_on_device(Ctx *c, std::vector<Job<T>> &jobs, const volatile 
   if ((rc = max_coresident_batch_blocks<T>(c, &max_blocks))) return rc;
   std::vector<int64_t> tiles((size_t)count), size((size_t)count);
   const int w = sizeof(T) == 8;
+  int largest_solo = 1;
   for (int i = 0; i < count; i++) {
     const PreparedLp &L = *jobs[i].L;
     tiles[i] = (int64_t)L.ntiles[w][0] + L.ntiles[w][1];
     size[i] = (int64_t)L.n + L.m + L.nnz;
+    largest_solo = std::max(largest_solo, team_blocks(L.n, L.m, max_blocks));
   }
-  const int tb = batch_team_blocks(tiles, max_blocks);
+  const int tb = batch_team_blocks(tiles, max_blocks, largest_solo);
   const int teams = std::min(count, max_blocks / tb);
   std::vector<int> order((size_t)count);
   for (int i = 0; i < count; i++) order[i] = i;

@@ -31,7 +31,11 @@ def test_device_search_matches_the_oracle_search(name, make, ints, optimum):
     else:
         assert dev.status == MilpStatus.OPTIMAL
         assert dev.objective_value == pytest.approx(optimum, abs=1e-6)
-        assert list(dev.primal) == list(ref.primal)
+        for j in range(len(dev.primal)):  # integer columns are snapped: exact; the rest to the LP tolerance
+            if j in ints:
+                assert dev.primal[j] == ref.primal[j]
+            else:
+                assert dev.primal[j] == pytest.approx(ref.primal[j], abs=1e-6)
 
 
 def test_device_search_on_the_16_item_knapsack():
