@@ -1,0 +1,266 @@
+"""Dispatch LOPF: a PyPSA network as an LP for the device solve, and the
+answer mapped back onto component names.  The dispatch subset of ``Lopf``
+(modules/network-lopf/src/main/scala/org/noaidi/lopf/Lopf.scala:69-561)
+with its conventions, since equivalence is judged against PyPSA's output:
+
+* columns per snapshot: each generator's output in p_nom x [p_min_pu,
+  p_max_pu], each passive branch's flow p0 in +-s_nom x s_max_pu, each link's
+  p0 in p_nom x [p_min_pu, p_max_pu]; costs are marginal_cost x the
+  snapshot's objective weighting (:148-196);
+* bus balance per snapshot and bus: generators inject, a branch takes p0 out
+  at bus0 and delivers efficiency x p0 at bus1 (1 for a line), loads on the
+  right-hand side (:281-333);
+* Kirchhoff's voltage law over a cycle basis of the passive branches, one
+  row per cycle per snapshot: sum(orientation x impedance x p0) = 0, with
+  reactance in AC sub-networks and resistance in DC ones, referred to
+  v_nom squared (:397-433; Cycles.scala);
+* primary-energy global constraints (<=): per generator, carrier intensity /
+  efficiency x the snapshot's generators weighting (:503-559).
+
+Components the dispatch model does not build (storage units, stores,
+transformers, processes, shunts) and extendable capacities are refused
+rather than dropped: a dropped component leaves a feasible LP for a
+different network.
+"""
+from __future__ import annotations
+
+import math
+from collections import deque
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from ..prima.model import LpBuilder, LpProblem, RowTranslation
+from ..prima.types import LpSolution, PdhgParams, SolveStatus
+from .pypsa_csv import Network
+
+HANDLED = {"Bus", "Carrier", "Generator", "Load", "Line", "Link", "GlobalConstraint", "SubNetwork", "LineType",
+           "Shape"}
+
+
+class UnsupportedNetwork(ValueError):
+    """``Lopf.UnsupportedNetwork``."""
+
+
+@dataclass
+class Cycle:
+    carrier: str
+    terms: list  # (component, id, orientation)
+
+
+@dataclass
+class Model:
+    problem: LpProblem
+    translation: RowTranslation
+    columns: dict      # (component, id, t) -> column
+    balance_rows: dict  # (bus, t) -> row of the builder's constraints (before standard form)
+    cycles: list
+
+
+@dataclass
+class LopfResult:
+    network: Network
+    model: Model
+    solution: LpSolution
+
+    @property
+    def status(self) -> SolveStatus:
+        return self.solution.status
+
+    @property
+    def objective(self) -> float:
+        return self.solution.objective_value
+
+    def dispatch(self, component: str, entity: str, t: int) -> float:
+        return float(self.solution.primal[self.model.columns[(component, entity, t)]])
+
+
+def _reject(network: Network) -> None:
+    unhandled = [f"{c} ({len(t)})" for c, t in network.tables.items() if len(t) and c not in HANDLED]
+    if unhandled:
+        raise UnsupportedNetwork("network contains unmodelled component(s): " + ", ".join(unhandled))
+    for comp, attr in (("Generator", "p_nom_extendable"), ("Link", "p_nom_extendable"), ("Line", "s_nom_extendable")):
+        tab = network.table(comp)
+        for i in tab.ids:
+            if bool(tab.value(attr, i)):
+                raise UnsupportedNetwork(f"{comp} '{i}' is extendable; capacity expansion is not in the dispatch model")
+    buses = set(network.table("Bus").ids)
+    for comp, ports in (("Generator", ("bus",)), ("Load", ("bus",)), ("Line", ("bus0", "bus1")),
+                        ("Link", ("bus0", "bus1"))):
+        tab = network.table(comp)
+        for i in tab.ids:
+            for port in ports:
+                if str(tab.value(port, i)) not in buses:
+                    raise UnsupportedNetwork(f"{comp} '{i}' references unknown bus '{tab.value(port, i)}' via {port}")
+
+
+def cycle_basis(network: Network) -> list:
+    """A cycle basis of the passive branches: per connected component a
+    breadth-first spanning tree and one cycle per non-tree edge (circuit rank
+    edges - nodes + components).  orientation +1 where the cycle runs bus0 to
+    bus1.  Any basis spans the same constraints."""
+    lines = network.table("Line")
+    edges = [("Line", i, str(lines.value("bus0", i)), str(lines.value("bus1", i))) for i in lines.ids]
+    adjacency: dict = {}
+    for e in edges:
+        adjacency.setdefault(e[2], []).append(e)
+        adjacency.setdefault(e[3], []).append(e)
+    bus_tab = network.table("Bus")
+    visited, cycles = set(), []
+    for root in bus_tab.ids:
+        if root in visited or root not in adjacency:
+            continue
+        carrier = str(bus_tab.value("carrier", root))
+        parent, depth = {}, {root: 0}
+        tree = set()
+        visited.add(root)
+        order = deque([root])
+        while order:
+            b = order.popleft()
+            for e in adjacency[b]:
+                nxt = e[3] if e[2] == b else e[2]
+                if nxt not in visited:
+                    visited.add(nxt)
+                    parent[nxt] = e
+                    depth[nxt] = depth[b] + 1
+                    tree.add((e[0], e[1]))
+                    order.append(nxt)
+        seen = set()
+        for b in sorted(depth):
+            for e in adjacency[b]:
+                key = (e[0], e[1])
+                if key in tree or key in seen:
+                    continue
+                seen.add(key)
+                # walk both ends up to their common ancestor: bus1 -> ... -> bus0 closes the cycle
+                terms = [(e[0], e[1], 1.0)]
+                a, c = e[3], e[2]
+                up_a, up_c = [], []
+                while depth[a] > depth[c]:
+                    p = parent[a]
+                    up_a.append((p[0], p[1], 1.0 if p[2] == a else -1.0))
+                    a = p[3] if p[2] == a else p[2]
+                while depth[c] > depth[a]:
+                    p = parent[c]
+                    up_c.append((p[0], p[1], 1.0 if p[3] == c else -1.0))
+                    c = p[3] if p[2] == c else p[2]
+                while a != c:
+                    p = parent[a]
+                    up_a.append((p[0], p[1], 1.0 if p[2] == a else -1.0))
+                    a = p[3] if p[2] == a else p[2]
+                    p = parent[c]
+                    up_c.append((p[0], p[1], 1.0 if p[3] == c else -1.0))
+                    c = p[3] if p[2] == c else p[2]
+                cycles.append(Cycle(carrier, terms + up_a + up_c))
+    return cycles
+
+
+def impedance(network: Network, component: str, entity: str, carrier: str) -> float:
+    """Reactance in an AC sub-network, resistance in a DC one, over v_nom^2 of bus0."""
+    tab = network.table(component)
+    raw = float(tab.value("r" if carrier == "DC" else "x", entity))
+    v = float(network.table("Bus").value("v_nom", str(tab.value("bus0", entity))))
+    return raw / (v * v)
+
+
+def build(network: Network) -> Model:
+    _reject(network)
+    T = len(network.snapshots)
+    if T == 0:
+        raise UnsupportedNetwork("network has no snapshots")
+    buses = network.table("Bus").ids
+    if not buses:
+        raise UnsupportedNetwork("network has no buses")
+    gens, lines, links, loads = (network.table(c) for c in ("Generator", "Line", "Link", "Load"))
+    columns, bounds, costs = {}, [], []
+
+    def declare(component, entity, t, lo, hi, cost):
+        columns[(component, entity, t)] = len(bounds)
+        bounds.append((lo, hi))
+        costs.append(cost)
+
+    for t in range(T):
+        w = network.weighting("objective", t)
+        for g in gens.ids:
+            pn = float(gens.value("p_nom", g))
+            lo, hi = pn * gens.at("p_min_pu", g, t), pn * gens.at("p_max_pu", g, t)
+            declare("Generator", g, t, min(lo, hi), max(lo, hi), gens.at("marginal_cost", g, t) * w)
+        for l in lines.ids:
+            lim = float(lines.value("s_nom", l)) * lines.at("s_max_pu", l, t)
+            declare("Line", l, t, -lim, lim, 0.0)
+        for k in links.ids:
+            pn = float(links.value("p_nom", k))
+            lo, hi = pn * links.at("p_min_pu", k, t), pn * links.at("p_max_pu", k, t)
+            declare("Link", k, t, min(lo, hi), max(lo, hi), links.at("marginal_cost", k, t) * w)
+
+    b = LpBuilder(len(bounds))
+    for j, (lo, hi) in enumerate(bounds):
+        b.bounds(j, lo, hi)
+    for j, c in enumerate(costs):
+        b.objective_coefficient(j, c)
+
+    balance_rows, row = {}, 0
+    for t in range(T):
+        for bus in buses:
+            terms = [(columns[("Generator", g, t)], 1.0) for g in gens.ids if str(gens.value("bus", g)) == bus]
+            for comp, tab in (("Line", lines), ("Link", links)):
+                for e in tab.ids:
+                    col = columns[(comp, e, t)]
+                    if str(tab.value("bus0", e)) == bus:
+                        terms.append((col, -1.0))
+                    if str(tab.value("bus1", e)) == bus:
+                        terms.append((col, 1.0 if comp == "Line" else tab.at("efficiency", e, t)))
+            demand = sum(loads.at("p_set", d, t) for d in loads.ids if str(loads.value("bus", d)) == bus)
+            b.equality_constraint(terms, demand)
+            balance_rows[(bus, t)] = row
+            row += 1
+
+    cycles = cycle_basis(network)
+    imp = {(c, e): impedance(network, c, e, cy.carrier) for cy in cycles for c, e, _ in cy.terms}
+    for cy in cycles:
+        if not any(imp[(c, e)] != 0.0 for c, e, _ in cy.terms):
+            raise UnsupportedNetwork("every branch in a cycle has zero impedance, so Kirchhoff's voltage law "
+                                     "would impose nothing on it")
+    for t in range(T):
+        for cy in cycles:
+            b.equality_constraint([(columns[(c, e, t)], o * imp[(c, e)]) for c, e, o in cy.terms], 0.0)
+
+    constraints = network.table("GlobalConstraint")
+    carriers = network.table("Carrier")
+    for gc in constraints.ids:
+        kind, sense = str(constraints.value("type", gc)), str(constraints.value("sense", gc))
+        if kind != "primary_energy":
+            raise UnsupportedNetwork(f"global constraint '{gc}' has type '{kind}'; only 'primary_energy' is implemented")
+        if sense != "<=":
+            raise UnsupportedNetwork(f"global constraint '{gc}' has sense '{sense}'; only '<=' is implemented")
+        attribute = str(constraints.value("carrier_attribute", gc))
+        terms = []
+        for t in range(T):
+            w = network.weighting("generators", t)
+            for g in gens.ids:
+                carrier = str(gens.value("carrier", g))
+                intensity = float(carriers.value(attribute, carrier)) if carrier in carriers.ids else 0.0
+                if not math.isfinite(intensity):
+                    intensity = 0.0
+                eff = gens.at("efficiency", g, t)
+                if intensity != 0.0 and eff != 0.0:
+                    terms.append((columns[("Generator", g, t)], intensity / eff * w))
+        if terms:
+            b.less_than(terms, float(constraints.value("constant", gc)))
+
+    problem, translation = b.build()
+    return Model(problem, translation, columns, balance_rows, cycles)
+
+
+def solve(network: Network, params: PdhgParams = PdhgParams(), precision: int = 64, device: int = 0,
+          mixed: bool = False, ctx=None) -> LopfResult:
+    """Build and solve on the GPU (``Lopf.solve``, :566-571); ``mixed`` runs
+    the FP32 refinement scheme instead of plain FP64 PDHG."""
+    from ..prima import cuda
+    model = build(network)
+    if mixed:
+        sol = cuda.mixed_solve(model.problem, params, ctx=ctx, device=device).solution
+    else:
+        sol = cuda.solve(model.problem, params, precision=precision, device=device, ctx=ctx)
+    return LopfResult(network, model, sol)

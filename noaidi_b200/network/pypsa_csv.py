@@ -1,0 +1,126 @@
+"""A PyPSA CSV network folder read into plain tables: the subset of the
+reference's network model (modules/network-model/.../CsvReader.scala,
+ComponentTable.scala) that the dispatch LOPF needs.
+
+A folder holds ``<list>.csv`` per component (one row per entity, the first
+column its name), ``<list>-<attribute>.csv`` for attributes that vary by
+snapshot (one row per snapshot, one column per entity), and
+``snapshots.csv`` with the weightings.  Attributes a file leaves out take
+PyPSA's defaults (the schema's ``default`` entries for the attributes used
+here); a varying attribute without a series file takes its static value.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+import pandas as pd
+
+# file stem of each component's tables (PyPSA's list names)
+LIST_NAMES = {
+    "Bus": "buses", "Carrier": "carriers", "Generator": "generators", "Load": "loads", "Line": "lines",
+    "Link": "links", "Transformer": "transformers", "StorageUnit": "storage_units", "Store": "stores",
+    "GlobalConstraint": "global_constraints", "SubNetwork": "sub_networks", "ShuntImpedance": "shunt_impedances",
+    "LineType": "line_types", "TransformerType": "transformer_types", "Shape": "shapes", "Process": "processes",
+}
+
+# PyPSA's defaults for the attributes the dispatch LOPF reads
+DEFAULTS = {
+    "Bus": {"v_nom": 1.0, "carrier": "AC"},
+    "Generator": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
+                  "p_nom_extendable": False, "carrier": ""},
+    "Load": {"p_set": 0.0},
+    "Line": {"x": 0.0, "r": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "s_nom_extendable": False},
+    "Link": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
+             "p_nom_extendable": False},
+    "GlobalConstraint": {"type": "primary_energy", "carrier_attribute": "co2_emissions", "sense": "=="},
+    "Carrier": {"co2_emissions": 0.0},
+}
+
+
+@dataclass
+class Table:
+    """One component's entities: static attributes and per-snapshot series."""
+    component: str
+    ids: list
+    static: dict = field(default_factory=dict)   # attribute -> {id: value}
+    series: dict = field(default_factory=dict)   # attribute -> array [snapshots, len(ids)]
+
+    def __len__(self) -> int:
+        return len(self.ids)
+
+    def has(self, attribute: str) -> bool:
+        return attribute in self.static or attribute in self.series
+
+    def value(self, attribute: str, entity: str):
+        """A static attribute (PyPSA's default when the file omits it)."""
+        if attribute in self.static:
+            v = self.static[attribute][entity]
+            if not (isinstance(v, float) and math.isnan(v)):
+                return v
+        return DEFAULTS.get(self.component, {}).get(attribute, math.nan)
+
+    def at(self, attribute: str, entity: str, t: int) -> float:
+        """A varying attribute at snapshot t: its series if there is one, else the static value."""
+        if attribute in self.series:
+            return float(self.series[attribute][t, self.ids.index(entity)])
+        return float(self.value(attribute, entity))
+
+
+@dataclass
+class Network:
+    name: str
+    snapshots: list
+    weightings: dict          # column of snapshots.csv -> array [snapshots]
+    tables: dict              # component -> Table
+
+    def table(self, component: str) -> Table:
+        return self.tables.get(component) or Table(component, [])
+
+    def weighting(self, column: str, t: int) -> float:
+        w = self.weightings.get(column)
+        return 1.0 if w is None else float(w[t])
+
+
+def _coerce(v):
+    if isinstance(v, (bool, np.bool_)):
+        return bool(v)
+    if isinstance(v, (int, float, np.integer, np.floating)):
+        return float(v)
+    if isinstance(v, str) and v.lower() in ("true", "false"):
+        return v.lower() == "true"
+    return v
+
+
+def read(folder: str, name: str = "") -> Network:
+    snap = pd.read_csv(os.path.join(folder, "snapshots.csv"))
+    label = "snapshot" if "snapshot" in snap.columns else snap.columns[0]
+    snapshots = list(snap[label])
+    weightings = {c: snap[c].to_numpy(dtype=np.float64) for c in ("objective", "stores", "generators")
+                  if c in snap.columns}
+    tables = {}
+    files = set(os.listdir(folder))
+    for component, stem in LIST_NAMES.items():
+        if f"{stem}.csv" not in files:
+            continue
+        df = pd.read_csv(os.path.join(folder, f"{stem}.csv"), keep_default_na=True)
+        if df.empty:
+            continue
+        ids = [str(v) for v in df[df.columns[0]]]
+        static = {col: {i: _coerce(v) for i, v in zip(ids, df[col])} for col in df.columns[1:]}
+        series = {}
+        for f in files:
+            if f.startswith(stem + "-") and f.endswith(".csv"):
+                attr = f[len(stem) + 1:-4]
+                s = pd.read_csv(os.path.join(folder, f), index_col=0)
+                arr = np.full((len(snapshots), len(ids)), math.nan)
+                for k, i in enumerate(ids):
+                    if i in s.columns:
+                        arr[:, k] = s[i].to_numpy(dtype=np.float64)
+                    else:
+                        arr[:, k] = float(Table(component, ids, static).value(attr, i))
+                series[attr] = arr
+        tables[component] = Table(component, ids, static, series)
+    return Network(name or os.path.basename(folder.rstrip("/")), snapshots, weightings, tables)

@@ -1,0 +1,37 @@
+"""Copies the input tables of PyPSA golden networks and the expected LOPF
+results (objective, generator dispatch, line flows) from the reference's
+goldens (reference/goldens/{networks,results} in oluies/noaidi, generated by
+PyPSA 1.2.4) into tests/golden/lopf/<network>/.
+
+    python tests/golden/make_lopf_fixtures.py [path to the reference checkout]
+"""
+import json
+import os
+import shutil
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+NETWORKS = ["ac-dc-dispatch"]
+# input tables only: component lists, their input series and the snapshots
+INPUTS = ["buses.csv", "carriers.csv", "generators.csv", "generators-p_max_pu.csv", "lines.csv", "links.csv",
+          "loads.csv", "loads-p_set.csv", "snapshots.csv", "global_constraints.csv"]
+
+
+def main(root):
+    goldens = os.path.join(root, "reference", "goldens")
+    for name in NETWORKS:
+        src = os.path.join(goldens, "networks", name)
+        dst = os.path.join(HERE, "lopf", name)
+        os.makedirs(dst, exist_ok=True)
+        for f in INPUTS:
+            if os.path.exists(os.path.join(src, f)):
+                shutil.copyfile(os.path.join(src, f), os.path.join(dst, f))
+        res = json.load(open(os.path.join(goldens, "results", f"{name}.json")))["optimize"]
+        keep = {k: res[k] for k in ("objective", "status", "condition", "generator_p", "line_p0", "link_p0")}
+        with open(os.path.join(dst, "expected.json"), "w") as f:
+            json.dump(keep, f, indent=1)
+        print(name, "->", dst)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,76 @@
+"""LopfSuite's golden checks (modules/network-lopf/src/test/scala/org/noaidi/
+lopf/LopfSuite.scala:115-220) on PyPSA's ac-dc-dispatch network: the LP
+built by noaidi_b200.network.lopf, solved by a solver passed in (the oracle
+on CPU, the device on GPU), against PyPSA's own optimum
+(tests/golden/lopf/, made by tests/golden/make_lopf_fixtures.py)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from noaidi_b200.network import lopf
+from noaidi_b200.network.pypsa_csv import read
+from noaidi_b200.prima import PdhgParams, SolveStatus
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "lopf")
+PARAMS = PdhgParams(eps_abs=1e-9, eps_rel=1e-9, max_iterations=500_000)
+
+
+def network(name="ac-dc-dispatch"):
+    return read(os.path.join(HERE, name), name)
+
+
+def expected(name="ac-dc-dispatch"):
+    return json.load(open(os.path.join(HERE, name, "expected.json")))
+
+
+def frame_value(frame, t, column):
+    v = frame["values"][t][frame["columns"].index(column)]
+    return float("nan") if isinstance(v, dict) else float(v)
+
+
+def check_against_pypsa(solve):
+    n = network()
+    exp = expected()
+    model = lopf.build(n)
+    sol = solve(model.problem)
+    res = lopf.LopfResult(n, model, sol)
+    assert res.status == SolveStatus.OPTIMAL
+    target = exp["objective"]
+    assert res.objective == pytest.approx(target, abs=1e-6 * max(1.0, abs(target)))
+    gens, lines, loads = n.table("Generator"), n.table("Line"), n.table("Load")
+    for t in range(len(n.snapshots)):
+        for g in gens.ids:
+            assert res.dispatch("Generator", g, t) == pytest.approx(frame_value(exp["generator_p"], t, g), abs=1e-3)
+        for l in lines.ids:
+            flow = res.dispatch("Line", l, t)
+            assert abs(flow) <= float(lines.value("s_nom", l)) + 1e-6
+            assert flow == pytest.approx(frame_value(exp["line_p0"], t, l), abs=1e-3)
+        generated = sum(res.dispatch("Generator", g, t) for g in gens.ids)
+        demanded = sum(loads.at("p_set", d, t) for d in loads.ids)
+        assert generated == pytest.approx(demanded, abs=1e-3)  # the links are lossless here
+    return res
+
+
+def check_cycle_rank():
+    n = network()
+    cycles = lopf.cycle_basis(n)
+    lines = n.table("Line")
+    buses = set()
+    for l in lines.ids:
+        buses.add(str(lines.value("bus0", l)))
+        buses.add(str(lines.value("bus1", l)))
+    # components of the passive graph
+    parent = {b: b for b in buses}
+
+    def find(b):
+        while parent[b] != b:
+            parent[b] = parent[parent[b]]
+            b = parent[b]
+        return b
+    for l in lines.ids:
+        parent[find(str(lines.value("bus0", l)))] = find(str(lines.value("bus1", l)))
+    components = len({find(b) for b in buses})
+    assert len(cycles) == len(lines.ids) - len(buses) + components
+    return cycles

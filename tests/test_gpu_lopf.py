@@ -1,0 +1,17 @@
+"""PyPSA's ac-dc-dispatch LOPF solved on the device, in FP64 and with the FP32
+refinement scheme, against PyPSA's optimum (LopfSuite.scala:115-207)."""
+import pytest
+
+from tests import lopf_cases as X
+
+pytestmark = pytest.mark.gpu
+
+
+def test_lopf_matches_pypsa_fp64_device():
+    from noaidi_b200.prima import cuda
+    X.check_against_pypsa(lambda p: cuda.solve(p, X.PARAMS, precision=64))
+
+
+def test_lopf_matches_pypsa_fp32_refinement():
+    from noaidi_b200.prima import cuda
+    X.check_against_pypsa(lambda p: cuda.mixed_solve(p, X.PARAMS).solution)
