@@ -18,9 +18,9 @@ with its conventions, since equivalence is judged against PyPSA's output:
   efficiency x the snapshot's generators weighting (:503-559).
 
 Components the dispatch model does not build (storage units, stores,
-transformers, processes, shunts) and extendable capacities are refused
-rather than dropped: a dropped component leaves a feasible LP for a
-different network.
+transformers, processes, shunts), extendable capacities, committable
+generators and generator set points are refused rather than dropped: a
+dropped component leaves a feasible LP for a different network.
 """
 from __future__ import annotations
 
@@ -85,6 +85,12 @@ def _reject(network: Network) -> None:
         for i in tab.ids:
             if bool(tab.value(attr, i)):
                 raise UnsupportedNetwork(f"{comp} '{i}' is extendable; capacity expansion is not in the dispatch model")
+    gens = network.table("Generator")
+    for g in gens.ids:
+        if bool(gens.value("committable", g)) is True:
+            raise UnsupportedNetwork(f"Generator '{g}' is committable; unit commitment is not a dispatch LP")
+    if "p_set" in gens.series and np.isfinite(gens.series["p_set"]).any():
+        raise UnsupportedNetwork("a generator has a p_set, which fixes its dispatch; the dispatch model does not")
     buses = set(network.table("Bus").ids)
     for comp, ports in (("Generator", ("bus",)), ("Load", ("bus",)), ("Line", ("bus0", "bus1")),
                         ("Link", ("bus0", "bus1"))):

@@ -30,7 +30,7 @@ LIST_NAMES = {
 DEFAULTS = {
     "Bus": {"v_nom": 1.0, "carrier": "AC"},
     "Generator": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
-                  "p_nom_extendable": False, "carrier": ""},
+                  "p_nom_extendable": False, "committable": False, "carrier": ""},
     "Load": {"p_set": 0.0},
     "Line": {"x": 0.0, "r": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "s_nom_extendable": False},
     "Link": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,

@@ -11,10 +11,11 @@ import shutil
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-NETWORKS = ["ac-dc-dispatch"]
+NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle"]
 # input tables only: component lists, their input series and the snapshots
-INPUTS = ["buses.csv", "carriers.csv", "generators.csv", "generators-p_max_pu.csv", "lines.csv", "links.csv",
-          "loads.csv", "loads-p_set.csv", "snapshots.csv", "global_constraints.csv"]
+INPUTS = ["buses.csv", "carriers.csv", "generators.csv", "generators-p_max_pu.csv", "generators-p_min_pu.csv",
+          "generators-marginal_cost.csv", "lines.csv", "links.csv", "loads.csv", "loads-p_set.csv", "snapshots.csv",
+          "global_constraints.csv"]
 
 
 def main(root):

@@ -30,9 +30,12 @@ def frame_value(frame, t, column):
     return float("nan") if isinstance(v, dict) else float(v)
 
 
-def check_against_pypsa(solve):
-    n = network()
-    exp = expected()
+NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle"]
+
+
+def check_against_pypsa(solve, name="ac-dc-dispatch"):
+    n = network(name)
+    exp = expected(name)
     model = lopf.build(n)
     sol = solve(model.problem)
     res = lopf.LopfResult(n, model, sol)
@@ -40,16 +43,22 @@ def check_against_pypsa(solve):
     target = exp["objective"]
     assert res.objective == pytest.approx(target, abs=1e-6 * max(1.0, abs(target)))
     gens, lines, loads = n.table("Generator"), n.table("Line"), n.table("Load")
+    # dispatch and flows are compared where the optimum is unique (the
+    # reference's LopfSuite does so on ac-dc-dispatch); elsewhere the objective
+    # and the ratings are what is determined
+    unique = name == "ac-dc-dispatch"
     for t in range(len(n.snapshots)):
-        for g in gens.ids:
+        for g in gens.ids if unique else ():
             assert res.dispatch("Generator", g, t) == pytest.approx(frame_value(exp["generator_p"], t, g), abs=1e-3)
         for l in lines.ids:
             flow = res.dispatch("Line", l, t)
-            assert abs(flow) <= float(lines.value("s_nom", l)) + 1e-6
-            assert flow == pytest.approx(frame_value(exp["line_p0"], t, l), abs=1e-3)
-        generated = sum(res.dispatch("Generator", g, t) for g in gens.ids)
-        demanded = sum(loads.at("p_set", d, t) for d in loads.ids)
-        assert generated == pytest.approx(demanded, abs=1e-3)  # the links are lossless here
+            assert abs(flow) <= float(lines.value("s_nom", l)) * lines.at("s_max_pu", l, t) + 1e-6
+            if unique:
+                assert flow == pytest.approx(frame_value(exp["line_p0"], t, l), abs=1e-3)
+        if not n.table("Link").ids:  # with no links, generation meets load at every snapshot
+            generated = sum(res.dispatch("Generator", g, t) for g in gens.ids)
+            demanded = sum(loads.at("p_set", d, t) for d in loads.ids)
+            assert generated == pytest.approx(demanded, abs=1e-3)
     return res
 
 

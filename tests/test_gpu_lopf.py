@@ -7,11 +7,13 @@ from tests import lopf_cases as X
 pytestmark = pytest.mark.gpu
 
 
-def test_lopf_matches_pypsa_fp64_device():
+@pytest.mark.parametrize("name", X.NETWORKS)
+def test_lopf_matches_pypsa_fp64_device(name):
     from noaidi_b200.prima import cuda
-    X.check_against_pypsa(lambda p: cuda.solve(p, X.PARAMS, precision=64))
+    X.check_against_pypsa(lambda p: cuda.solve(p, X.PARAMS, precision=64), name)
 
 
-def test_lopf_matches_pypsa_fp32_refinement():
+@pytest.mark.parametrize("name", X.NETWORKS)
+def test_lopf_matches_pypsa_fp32_refinement(name):
     from noaidi_b200.prima import cuda
-    X.check_against_pypsa(lambda p: cuda.mixed_solve(p, X.PARAMS).solution)
+    X.check_against_pypsa(lambda p: cuda.mixed_solve(p, X.PARAMS).solution, name)

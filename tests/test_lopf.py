@@ -6,9 +6,10 @@ from noaidi_b200.network import lopf
 from tests import lopf_cases as X
 
 
-def test_lopf_matches_pypsa_with_the_oracle():
+@pytest.mark.parametrize("name", X.NETWORKS)
+def test_lopf_matches_pypsa_with_the_oracle(name):
     from oracle import oracle as O
-    X.check_against_pypsa(lambda p: O.solve(p, X.PARAMS))
+    X.check_against_pypsa(lambda p: O.solve(p, X.PARAMS), name)
 
 
 def test_cycle_basis_has_the_circuit_rank():
