@@ -131,22 +131,25 @@ struct None {};
 #ifndef PRIMA_HOT_F32_CAP
 #define PRIMA_HOT_F32_CAP 2048
 #define PRIMA_HOT_F32_STAGES 2
+#define PRIMA_HOT_F32_RPT 2
 #endif
 #ifndef PRIMA_HOT_F64_CAP
-#define PRIMA_HOT_F64_CAP 1024
+#define PRIMA_HOT_F64_CAP 1536
 #define PRIMA_HOT_F64_STAGES 2
+#define PRIMA_HOT_F64_RPT 2
 #endif
-template <int C, int S>
+template <int C, int S, int R>
 struct HotShape {
-  static constexpr int kCap = C, kStages = S;
+  static constexpr int kCap = C, kStages = S, kRowsPerThread = R;
 };
 template <typename T>
 struct Hot;
 template <>
-struct Hot<float> : HotShape<PRIMA_HOT_F32_CAP, PRIMA_HOT_F32_STAGES> {};
+struct Hot<float> : HotShape<PRIMA_HOT_F32_CAP, PRIMA_HOT_F32_STAGES, PRIMA_HOT_F32_RPT> {};
 template <>
-struct Hot<double> : HotShape<PRIMA_HOT_F64_CAP, PRIMA_HOT_F64_STAGES> {};
-constexpr int kHotRows = kThreads;  // rows per tile, at most: one per thread
+struct Hot<double> : HotShape<PRIMA_HOT_F64_CAP, PRIMA_HOT_F64_STAGES, PRIMA_HOT_F64_RPT> {};
+template <typename T>
+constexpr int kHotRows = kThreads * Hot<T>::kRowsPerThread;  // rows per tile, at most
 constexpr int kHotVec = 6;          // vector slices per tile, at most
 constexpr int kHotBatch = 128;      // tiles whose table entries a block stages at once
 constexpr int kMaxStages = Hot<float>::kStages > Hot<double>::kStages ? Hot<float>::kStages : Hot<double>::kStages;
@@ -155,11 +158,11 @@ template <typename T>
 struct HotLayout {
   static constexpr int kCap = Hot<T>::kCap;  // staged nonzeros (16-byte rounded span)
   static constexpr int kStages = Hot<T>::kStages;
-  static constexpr size_t rp_bytes = ((size_t)(kHotRows + 1) * 4 + 15) / 16 * 16;
+  static constexpr size_t rp_bytes = ((size_t)(kHotRows<T> + 1) * 4 + 15) / 16 * 16;
   static constexpr size_t ci_off = rp_bytes;
   static constexpr size_t v_off = ci_off + (size_t)kCap * 4;
   static constexpr size_t vec_off = (v_off + (size_t)kCap * sizeof(T) + 15) / 16 * 16;
-  static constexpr size_t vec_stride = (size_t)kHotRows * sizeof(T);
+  static constexpr size_t vec_stride = (size_t)kHotRows<T> * sizeof(T);
   static constexpr size_t stage_bytes = (vec_off + kHotVec * vec_stride + 127) / 128 * 128;
   static constexpr size_t total = kStages * stage_bytes;
 };
@@ -284,35 +287,62 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
       const T *slices = reinterpret_cast<const T *>(buf + L::vec_off);
       const int32_t ka = e0.y & ~3;
       const bool staged = spmv && ((e1.y + 3) & ~3) - ka <= L::kCap;
-      const int i = threadIdx.x;
-      if (i < rows) {
-        T acc = T(0);
-        if (spmv) {
-          const int32_t a0 = rp_s[i], a1 = rp_s[i + 1];
-          if (staged) {  // four gathers in flight; the sum stays in index order
-            int32_t k = a0;
-            for (; k + 4 <= a1; k += 4) {
-              const int32_t c0 = ci_s[k - ka], c1 = ci_s[k + 1 - ka], c2 = ci_s[k + 2 - ka], c3 = ci_s[k + 3 - ka];
-              const T x0 = ldv(xg + c0), x1 = ldv(xg + c1), x2 = ldv(xg + c2), x3 = ldv(xg + c3);
-              acc = acc + (v_s[k - ka] * x0);
-              acc = acc + (v_s[k + 1 - ka] * x1);
-              acc = acc + (v_s[k + 2 - ka] * x2);
-              acc = acc + (v_s[k + 3 - ka] * x3);
-            }
-            const int rem = a1 - k;
-            if (rem > 0) {
-              const int32_t c0 = ci_s[k - ka];
-              const int32_t c1 = rem > 1 ? ci_s[k + 1 - ka] : c0, c2 = rem > 2 ? ci_s[k + 2 - ka] : c0;
-              const T x0 = ldv(xg + c0), x1 = ldv(xg + c1), x2 = ldv(xg + c2);
-              acc = acc + (v_s[k - ka] * x0);
-              if (rem > 1) acc = acc + (v_s[k + 1 - ka] * x1);
-              if (rem > 2) acc = acc + (v_s[k + 2 - ka] * x2);
-            }
+      // each thread takes rows threadIdx.x + r * kThreads of the tile; the
+      // first four gathers of all its rows are issued together
+      constexpr int RPT = Hot<T>::kRowsPerThread;
+      T acc[RPT];
+      int32_t a0[RPT], a1[RPT];
+#pragma unroll
+      for (int q = 0; q < RPT; q++) {
+        const int i = threadIdx.x + q * kThreads;
+        acc[q] = T(0);
+        a0[q] = a1[q] = 0;
+        if (spmv && i < rows) {
+          if (staged) {
+            a0[q] = rp_s[i];
+            a1[q] = rp_s[i + 1];
           } else {
-            for (int32_t k = a0; k < a1; k++) acc = acc + (__ldg(v + k) * ldv(xg + __ldg(ci + k)));
+            a0[q] = __ldg(rp + r0 + i);
+            a1[q] = __ldg(rp + r0 + i + 1);
           }
         }
-        epi(r0 + i, i, acc, slices);
+      }
+      if (staged) {  // index-order sums: the first four products of every row, then the rest four at a time
+        int32_t col[RPT][4];
+        T x[RPT][4];
+#pragma unroll
+        for (int q = 0; q < RPT; q++)
+#pragma unroll
+          for (int u = 0; u < 4; u++) col[q][u] = a0[q] + u < a1[q] ? ci_s[a0[q] + u - ka] : -1;
+#pragma unroll
+        for (int q = 0; q < RPT; q++)
+#pragma unroll
+          for (int u = 0; u < 4; u++) x[q][u] = col[q][u] >= 0 ? ldv(xg + col[q][u]) : T(0);
+#pragma unroll
+        for (int q = 0; q < RPT; q++) {
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (a0[q] + u < a1[q]) acc[q] = acc[q] + (v_s[a0[q] + u - ka] * x[q][u]);
+          int32_t k = a0[q] + 4;
+          for (; k + 4 <= a1[q]; k += 4) {
+            const int32_t c0 = ci_s[k - ka], c1 = ci_s[k + 1 - ka], c2 = ci_s[k + 2 - ka], c3 = ci_s[k + 3 - ka];
+            const T x0 = ldv(xg + c0), x1 = ldv(xg + c1), x2 = ldv(xg + c2), x3 = ldv(xg + c3);
+            acc[q] = acc[q] + (v_s[k - ka] * x0);
+            acc[q] = acc[q] + (v_s[k + 1 - ka] * x1);
+            acc[q] = acc[q] + (v_s[k + 2 - ka] * x2);
+            acc[q] = acc[q] + (v_s[k + 3 - ka] * x3);
+          }
+          for (; k < a1[q]; k++) acc[q] = acc[q] + (v_s[k - ka] * ldv(xg + ci_s[k - ka]));
+        }
+      } else if (spmv) {
+#pragma unroll
+        for (int q = 0; q < RPT; q++)
+          for (int32_t k = a0[q]; k < a1[q]; k++) acc[q] = acc[q] + (__ldg(v + k) * ldv(xg + __ldg(ci + k)));
+      }
+#pragma unroll
+      for (int q = 0; q < RPT; q++) {
+        const int i = threadIdx.x + q * kThreads;
+        if (i < rows) epi(r0 + i, i, acc[q], slices);
       }
       // the last warp done with this stage refills it with the tile S further on
       __syncwarp();
@@ -732,7 +762,7 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
     const T *vecs[6] = {x, a.sx, a.skty, a.c, a.l, a.u};
     ok = hot_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], vecs, 6, smem, hs, par,
                       &a.sync->abort, [&](int32_t j, int i, T kt, const T *sl) {
-                        constexpr int S = kHotRows;
+                        constexpr int S = kHotRows<T>;
                         const T xj = sl[i], sx = sl[S + i], skt = sl[2 * S + i];
                         const T cj = sl[3 * S + i], lj = sl[4 * S + i], uj = sl[5 * S + i];
                         a.kty[j] = kt;
@@ -744,7 +774,7 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
     const T *vecs[5] = {x, a.kty, a.c, a.l, a.u};
     ok = hot_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, nullptr, nullptr, nullptr, nullptr, vecs, 5, smem, hs, par,
                       &a.sync->abort, [&](int32_t j, int i, T, const T *sl) {
-                        constexpr int S = kHotRows;
+                        constexpr int S = kHotRows<T>;
                         step(j, sl[i], sl[S + i], sl[2 * S + i], sl[3 * S + i], sl[4 * S + i]);
                       });
   }
@@ -775,7 +805,7 @@ __device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsi
   const bool has_lo = a.ylo != nullptr;
   const bool ok = hot_tiles<T>(a.ntiles_k, tm.nb, tm.rank, a.tiles_k, a.kp, a.kci, a.kv, (const T *)a.xbar, vecs, nv, smem, hs, par,
                                &a.sync->abort, [&](int32_t r, int i, T kb, const T *sl) {
-    constexpr int S = kHotRows;
+    constexpr int S = kHotRows<T>;
     const T yr = sl[i], kxr = sl[S + i], qr = sl[2 * S + i];
     const T syr = pend ? sl[3 * S + i] : T(0), skxr = pend ? sl[4 * S + i] : T(0);
     const T lb = has_lo ? sl[iylo * S + i] : T(0);
@@ -1312,7 +1342,7 @@ __device__ __forceinline__ void init_stages(HotShared &hs) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, kMinBlocksPerSm) pdhg_kernel(Args<T> a) {
+__global__ void __launch_bounds__(kThreads, kMinBlocksPerSm<T>) pdhg_kernel(Args<T> a) {
   __shared__ Control snap;
   __shared__ double s_part[kMaxQ];
   __shared__ HotShared hs;
@@ -1330,7 +1360,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksPerSm) pdhg_kernel(Args<T>
 // instance has its own Control, Sync and state; a team runs exactly the
 // single-solve phase machine on it.
 template <typename T>
-__global__ void __launch_bounds__(kThreads, kMinBlocksPerSm)
+__global__ void __launch_bounds__(kThreads, kMinBlocksPerSm<T>)
     pdhg_batch_kernel(const Args<T> *__restrict__ args, int count, int tb, int32_t *queue, int32_t *team_next) {
   __shared__ Control snap;
   __shared__ double s_part[kMaxQ];
@@ -1472,7 +1502,7 @@ std::vector<int2> tile_table(const std::vector<int32_t> &rp) {
   while (r < rows) {
     table.push_back(make_int2((int)r, rp[r]));
     int64_t e = r;
-    while (e < rows && e - r < dev::kHotRows) {
+    while (e < rows && e - r < dev::kHotRows<T>) {
       const int64_t e2 = std::min<int64_t>(rows, e + 4);
       if (e > r && (((int64_t)rp[e2] + 3) & ~3) - (rp[r] & ~3) > cap) break;
       e = e2;

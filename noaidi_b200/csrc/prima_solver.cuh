@@ -40,10 +40,18 @@ namespace dev {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-#ifndef PRIMA_MIN_BLOCKS_PER_SM
-#define PRIMA_MIN_BLOCKS_PER_SM 4
+// Blocks per SM the solver kernel is compiled for (its register budget):
+// three in FP32 (80 registers), two in FP64 (128), each thread owning two
+// rows of a tile -- measured faster than four blocks at 64 registers, where
+// the cold phases spilled and each thread had one row's gathers in flight.
+#ifndef PRIMA_MIN_BLOCKS_F32
+#define PRIMA_MIN_BLOCKS_F32 3
 #endif
-constexpr int kMinBlocksPerSm = PRIMA_MIN_BLOCKS_PER_SM;  // register cap 64: enough warps in flight for the gathers
+#ifndef PRIMA_MIN_BLOCKS_F64
+#define PRIMA_MIN_BLOCKS_F64 2
+#endif
+template <typename T>
+constexpr int kMinBlocksPerSm = sizeof(T) == 4 ? PRIMA_MIN_BLOCKS_F32 : PRIMA_MIN_BLOCKS_F64;
 constexpr int kTileRows = 512;      // rows of one CSR-stream tile (2 per thread)
 constexpr int kRowsPerThread = kTileRows / kThreads;
 constexpr int kTileCap = 4096;      // staged products per tile (dynamic shared memory)
