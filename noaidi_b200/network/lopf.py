@@ -31,7 +31,7 @@ from typing import Optional
 
 import numpy as np
 
-from ..prima.model import LpBuilder, LpProblem, RowTranslation
+from ..prima.model import LpBuilder, LpProblem, Negated, RowTranslation
 from ..prima.types import LpSolution, PdhgParams, SolveStatus
 from .pypsa_csv import Network
 
@@ -270,3 +270,134 @@ def solve(network: Network, params: PdhgParams = PdhgParams(), precision: int = 
     else:
         sol = cuda.solve(model.problem, params, precision=precision, device=device, ctx=ctx)
     return LopfResult(network, model, sol)
+
+
+# ---- security-constrained LOPF (N-1) ------------------------------------------
+
+def sub_networks(network: Network) -> list:
+    """Connected components of the buses over the passive branches, each
+    (carrier, [buses], [line ids]) -- ``Topology.subNetworks``."""
+    lines = network.table("Line")
+    bus_tab = network.table("Bus")
+    adjacency: dict = {b: [] for b in bus_tab.ids}
+    for l in lines.ids:
+        b0, b1 = str(lines.value("bus0", l)), str(lines.value("bus1", l))
+        adjacency[b0].append((l, b1))
+        adjacency[b1].append((l, b0))
+    seen, out = set(), []
+    for root in bus_tab.ids:
+        if root in seen:
+            continue
+        comp, stack, lids = [], [root], set()
+        seen.add(root)
+        while stack:
+            b = stack.pop()
+            comp.append(b)
+            for l, nb in adjacency[b]:
+                lids.add(l)
+                if nb not in seen:
+                    seen.add(nb)
+                    stack.append(nb)
+        out.append((str(bus_tab.value("carrier", root)), comp, [l for l in lines.ids if l in lids]))
+    return out
+
+
+def lodf(network: Network, carrier: str, buses: list, lines: list, outages: Optional[set] = None):
+    """Line outage distribution factors of one sub-network (``Lodf.of``,
+    modules/network-pf/.../Lodf.scala): PTDF = diag(b) A B^-1 with the first
+    bus as reference (the factors do not depend on that choice), and
+    LODF[l, o] = PTDF_l(o) / (1 - PTDF_o(o)), -1 on the diagonal.  A bridge
+    (a denominator within 1e-7 of zero) has no post-outage flow: it is
+    refused if requested as a contingency and left unpopulated otherwise.
+    Returns (lines, factors m x m, populated per outage column)."""
+    m = len(lines)
+    if m == 0:
+        return [], np.zeros((0, 0)), np.zeros(0, dtype=bool)
+    tab = network.table("Line")
+    index = {b: i for i, b in enumerate(buses[1:])}
+    n = len(index)
+    y = np.array([1.0 / impedance(network, "Line", l, carrier) for l in lines])
+    A = np.zeros((m, n))
+    for k, l in enumerate(lines):
+        b0, b1 = str(tab.value("bus0", l)), str(tab.value("bus1", l))
+        if b0 in index:
+            A[k, index[b0]] += 1.0
+        if b1 in index:
+            A[k, index[b1]] -= 1.0
+    B = A.T @ (y[:, None] * A)
+    try:
+        np.linalg.cholesky(B)
+    except np.linalg.LinAlgError as e:
+        raise UnsupportedNetwork(f"sub-network {buses} has no unique power flow: {e}") from None
+    ptdf = (y[:, None] * A) @ np.linalg.inv(B)       # [m lines, n buses]
+    branch_ptdf = ptdf @ A.T                           # [m, m]: flow on l per unit shifted across o
+    factors = np.zeros((m, m))
+    populated = np.zeros(m, dtype=bool)
+    for j, l in enumerate(lines):
+        denominator = 1.0 - branch_ptdf[j, j]
+        requested = outages is None or l in outages
+        if abs(denominator) < 1e-7:
+            if requested:
+                raise UnsupportedNetwork(f"Line '{l}' is a bridge: removing it disconnects the sub-network, "
+                                         "so it is not a credible contingency")
+            continue
+        populated[j] = True
+        factors[:, j] = branch_ptdf[:, j] / denominator
+        factors[j, j] = -1.0
+    return lines, factors, populated
+
+
+def build_sclopf(network: Network, outages: Optional[list] = None) -> Model:
+    """``Sclopf.build`` (modules/network-lopf/.../Sclopf.scala:80-239): the
+    dispatch LP plus, per snapshot, monitored line l and contingency o != l
+    with a non-zero factor, the rating row
+    -s_nom_l s_max_pu <= f_l + LODF[l, o] f_o <= s_nom_l s_max_pu.
+    ``outages`` defaults to every line."""
+    base = build(network)
+    if outages is not None and not outages:
+        return base
+    lines_tab = network.table("Line")
+    subs = [(carrier, buses, lines, lodf(network, carrier, buses, lines, None if outages is None else set(outages)))
+            for carrier, buses, lines in sub_networks(network)]
+    requested = list(lines_tab.ids) if outages is None else list(outages)
+    for o in requested:
+        if o not in lines_tab.ids:
+            raise UnsupportedNetwork(f"'{o}' is not a passive branch of this network, so it cannot be a contingency")
+    where = {}
+    for s_idx, (_, _, lines, (names, factors, populated)) in enumerate(subs):
+        for k, l in enumerate(names):
+            where[l] = (s_idx, k)
+    p = base.problem
+    b = LpBuilder(p.num_variables)
+    for j in range(p.num_variables):
+        b.bounds(j, float(p.variable_lower[j]), float(p.variable_upper[j]))
+        b.objective_coefficient(j, float(p.objective[j]))
+    b.objective_offset(p.objective_offset)
+    K = p.constraint_matrix
+    # standard-form rows that came from a <= row (copied back as <= rows)
+    negated = {base.translation.expansion_of(r).row for r in range(base.translation.num_original_rows)
+               if isinstance(base.translation.expansion_of(r), Negated)}
+    for r in range(p.num_constraints):
+        a, e = K.row_ptr[r], K.row_ptr[r + 1]
+        terms = [(int(c), float(v)) for c, v in zip(K.col_indices[a:e], K.values[a:e])]
+        q = float(p.rhs[r])
+        if r < p.num_equalities:
+            b.equality_constraint(terms, q)
+        elif r in negated:
+            b.less_than([(c, -v) for c, v in terms], -q)
+        else:
+            b.greater_than(terms, q)
+    for t in range(len(network.snapshots)):
+        for s_idx, (_, _, lines, (names, factors, populated)) in enumerate(subs):
+            for k, l in enumerate(names):
+                limit = float(lines_tab.value("s_nom", l)) * lines_tab.at("s_max_pu", l, t)
+                col = base.columns[("Line", l, t)]
+                for o in requested:
+                    if o == l or where.get(o, (None,))[0] != s_idx:
+                        continue
+                    j = where[o][1]
+                    factor = float(factors[k, j]) if populated[j] else 0.0
+                    if factor != 0.0:
+                        b.constraint([(col, 1.0), (base.columns[("Line", o, t)], factor)], -limit, limit)
+    problem, translation = b.build()
+    return Model(problem, translation, base.columns, base.balance_rows, base.cycles)

@@ -83,3 +83,18 @@ def check_cycle_rank():
     components = len({find(b) for b in buses})
     assert len(cycles) == len(lines.ids) - len(buses) + components
     return cycles
+
+
+def check_sclopf_triangle(solve):
+    """SclopfSuite on sclopf-triangle: PyPSA's secure optimum 14100 (the plain
+    one is 6900) with the outages PyPSA used, dispatch within 1e-3 MW."""
+    n = network("sclopf-triangle")
+    exp = expected("sclopf-triangle")["sclopf"]
+    model = lopf.build_sclopf(n, exp["branch_outages"])
+    res = lopf.LopfResult(n, model, solve(model.problem))
+    assert res.status == SolveStatus.OPTIMAL
+    assert res.objective == pytest.approx(exp["objective"], abs=1e-6 * abs(exp["objective"]))
+    for t in range(len(n.snapshots)):
+        for g in n.table("Generator").ids:
+            assert res.dispatch("Generator", g, t) == pytest.approx(frame_value(exp["generator_p"], t, g), abs=1e-3)
+    return res

@@ -17,3 +17,9 @@ def test_lopf_matches_pypsa_fp64_device(name):
 def test_lopf_matches_pypsa_fp32_refinement(name):
     from noaidi_b200.prima import cuda
     X.check_against_pypsa(lambda p: cuda.mixed_solve(p, X.PARAMS).solution, name)
+
+
+def test_sclopf_matches_pypsa_on_the_device():
+    from noaidi_b200.prima import cuda
+    X.check_sclopf_triangle(lambda p: cuda.solve(p, X.PARAMS, precision=64))
+    X.check_sclopf_triangle(lambda p: cuda.mixed_solve(p, X.PARAMS).solution)
