@@ -141,3 +141,91 @@ def lopf_batch(seed: int = 0, count: int = 256, min_buses: int = 100, max_buses:
         scale = float(rng.uniform(0.6, 0.95))
         out.append(dc_lopf(seed + i, B, (3 * B) // 2, B // 2, T, scale))
     return out
+
+
+def lodf_matrix(net: Network) -> tuple[np.ndarray, np.ndarray]:
+    """Line outage distribution factors of a connected network (susceptance
+    1/x, bus 0 as reference): LODF[l, o] = PTDF_l(o) / (1 - PTDF_o(o)) with
+    -1 on the diagonal, and a mask of the lines that are not bridges."""
+    B, L = net.buses, net.lines
+    A = np.zeros((L, B - 1))
+    idx = np.arange(L)
+    f, t = net.line_from, net.line_to
+    A[idx[f > 0], f[f > 0] - 1] += 1.0
+    A[idx[t > 0], t[t > 0] - 1] -= 1.0
+    y = 1.0 / net.reactance
+    ptdf = (y[:, None] * A) @ np.linalg.inv(A.T @ (y[:, None] * A))
+    branch = ptdf @ A.T
+    denominator = 1.0 - np.diag(branch)
+    ok = np.abs(denominator) >= 1e-7
+    lodf = np.zeros((L, L))
+    lodf[:, ok] = branch[:, ok] / denominator[ok]
+    np.fill_diagonal(lodf, -1.0)
+    return lodf, ok
+
+
+def sclopf_n1(seed: int = 0, buses: int = 500, lines: int = 750, generators: int = 300, snapshots: int = 24,
+              outages: int = 200, load_scale: float = 0.7, voll: float = 1000.0) -> LpProblem:
+    """N-1 security-constrained DC-LOPF (config 4): ``dc_lopf`` on a
+    spanning tree plus chords, and for every snapshot, monitored line l and
+    contingency o != l with a non-zero factor, the rating range
+    ``-s_nom_l <= f_l + LODF[l, o] f_o <= s_nom_l`` -- the reference's
+    formulation (Sclopf.scala:215-236), two standard-form rows of two
+    nonzeros each.  The contingencies are the ``outages`` non-bridge lines
+    carrying the most flow in a DC power flow of the average hour with
+    generators dispatched in proportion to availability (a seeded stand-in
+    for ranking by a base solve)."""
+    rng = np.random.default_rng(seed)
+    net = random_network(rng, buses, lines, generators)
+    base = dc_lopf(seed, buses, lines, generators, snapshots, load_scale, network=net, voll=voll)
+    # the same draws dc_lopf made after the network, for the ranking flow
+    rng2 = np.random.default_rng(seed)
+    random_network(rng2, buses, lines, generators)
+    avail = rng2.uniform(0.3, 1.0, (snapshots, generators))
+    load = rng2.lognormal(3.0, 0.5, (snapshots, buses))
+    load *= (load_scale * (avail * net.p_nom).sum(axis=1) / load.sum(axis=1))[:, None]
+    lodf, ok = lodf_matrix(net)
+    inj = np.zeros(buses)
+    gen = (avail * net.p_nom).mean(axis=0)
+    np.add.at(inj, net.gen_bus, gen * load.mean(axis=0).sum() / gen.sum())
+    inj -= load.mean(axis=0)
+    A = np.zeros((net.lines, buses - 1))
+    idx = np.arange(net.lines)
+    f, t = net.line_from, net.line_to
+    A[idx[f > 0], f[f > 0] - 1] += 1.0
+    A[idx[t > 0], t[t > 0] - 1] -= 1.0
+    y = 1.0 / net.reactance
+    flow = (y[:, None] * A) @ np.linalg.solve(A.T @ (y[:, None] * A), inj[1:])
+    candidates = np.flatnonzero(ok)
+    chosen = candidates[np.argsort(-np.abs(flow[candidates]), kind="stable")[:outages]]
+    chosen.sort()
+    # security pairs (l, o) with a non-zero factor, the same every snapshot
+    ll, oo = np.nonzero(lodf[:, chosen] != 0.0)
+    oo = chosen[oo]
+    keep = ll != oo
+    ll, oo = ll[keep], oo[keep]
+    F = lodf[ll, oo]
+    G, L, Bn, T = generators, net.lines, buses, snapshots
+    nv = G + 2 * Bn + L
+    F0 = G + Bn
+    P = ll.size
+    t_idx = np.repeat(np.arange(T), P)
+    cl = (t_idx * nv + F0 + np.tile(ll, T))
+    co = (t_idx * nv + F0 + np.tile(oo, T))
+    fv = np.tile(F, T)
+    lim = np.tile(net.s_nom[ll], T)
+    # two rows per pair: (f_l + F f_o >= -s) and (-f_l - F f_o >= -s); columns ascending within a row
+    first = np.minimum(cl, co)
+    second = np.maximum(cl, co)
+    a_first = np.where(cl < co, 1.0, fv)
+    a_second = np.where(cl < co, fv, 1.0)
+    nrows = 2 * P * T
+    sec_cols = np.stack([first, second, first, second], axis=1).reshape(-1, 2)
+    sec_vals = np.stack([a_first, a_second, -a_first, -a_second], axis=1).reshape(-1, 2)
+    K0 = base.constraint_matrix
+    rp = np.concatenate([K0.row_ptr, K0.nnz + 2 * np.arange(1, nrows + 1)])
+    ci = np.concatenate([K0.col_indices, sec_cols.ravel()])
+    vv = np.concatenate([K0.values, sec_vals.ravel()])
+    K = SparseMatrix(K0.rows + nrows, K0.cols, rp, ci, vv)
+    q = np.concatenate([base.rhs, -np.repeat(lim, 2)])
+    return LpProblem(base.objective, K, q, base.num_equalities, base.variable_lower, base.variable_upper)
