@@ -140,6 +140,7 @@ struct None {};
 #endif
 template <int C, int S, int R>
 struct HotShape {
+  static_assert(C % 4 == 0 && C / 4 >= 32, "an unstaged tile splits the value area among its up to 4 rows");
   static constexpr int kCap = C, kStages = S, kRowsPerThread = R;
 };
 template <typename T>
@@ -301,13 +302,40 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
           if (staged) {
             a0[q] = rp_s[i];
             a1[q] = rp_s[i + 1];
-          } else {
-            a0[q] = __ldg(rp + r0 + i);
-            a1[q] = __ldg(rp + r0 + i + 1);
           }
         }
       }
-      if (staged) {  // index-order sums: the first four products of every row, then the rest four at a time
+      const bool dense = staged && (int64_t)(e1.y - e0.y) > 8 * (int64_t)rows;
+      if (dense) {
+        // Long rows: the warp first forms the products of its rows' nonzeros
+        // in place in the stage (lanes side by side, four gathers each in
+        // flight), then each thread sums its rows from shared memory in
+        // index order.  A thread walking a 400-nonzero row four gathers at a
+        // time would wait a hundred round trips.
+        T *vw = const_cast<T *>(v_s);
+#pragma unroll
+        for (int q = 0; q < RPT; q++) {
+          const int rlo = q * kThreads + (threadIdx.x & ~31);
+          if (rlo < rows) {
+            const int32_t k0 = rp_s[rlo], k1 = rp_s[min(rows, rlo + 32)];
+            for (int32_t k = k0 + lane; k < k1; k += 4 * 32) {
+              int32_t cc[4];
+              T xx[4];
+#pragma unroll
+              for (int u = 0; u < 4; u++) cc[u] = k + u * 32 < k1 ? ci_s[k + u * 32 - ka] : -1;
+#pragma unroll
+              for (int u = 0; u < 4; u++) xx[u] = cc[u] >= 0 ? ldv(xg + cc[u]) : T(0);
+#pragma unroll
+              for (int u = 0; u < 4; u++)
+                if (cc[u] >= 0) vw[k + u * 32 - ka] = vw[k + u * 32 - ka] * xx[u];
+            }
+          }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < RPT; q++)
+          for (int32_t k = a0[q]; k < a1[q]; k++) acc[q] = acc[q] + vw[k - ka];
+      } else if (staged) {  // index-order sums: the first four products of every row, then the rest four at a time
         int32_t col[RPT][4];
         T x[RPT][4];
 #pragma unroll
@@ -334,15 +362,36 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
           }
           for (; k < a1[q]; k++) acc[q] = acc[q] + (v_s[k - ka] * ldv(xg + ci_s[k - ka]));
         }
-      } else if (spmv) {
-#pragma unroll
-        for (int q = 0; q < RPT; q++)
-          for (int32_t k = a0[q]; k < a1[q]; k++) acc[q] = acc[q] + (__ldg(v + k) * ldv(xg + __ldg(ci + k)));
       }
+      if (spmv && !staged) {
+        // A tile whose nonzeros do not fit a stage is one group of at most 4
+        // long rows (a dense column of K, say).  Warp w takes row w: its
+        // lanes form the products in chunks into the stage's value area,
+        // which this tile leaves unused, and lane 0 sums each chunk in index
+        // order -- the same sum as everywhere else, without one thread
+        // walking thousands of dependent loads.
+        constexpr int kChunk = L::kCap / 4;
+        const int w = threadIdx.x >> 5;
+        T accw = T(0);
+        if (w < rows) {
+          T *scratch = reinterpret_cast<T *>(const_cast<unsigned char *>(buf) + L::v_off) + w * kChunk;
+          const int32_t b0 = __ldg(rp + r0 + w), b1 = __ldg(rp + r0 + w + 1);
+          for (int32_t base = b0; base < b1; base += kChunk) {
+            const int32_t cnt = min(kChunk, b1 - base);
+            for (int32_t k = lane; k < cnt; k += 32) scratch[k] = __ldg(v + base + k) * ldv(xg + __ldg(ci + base + k));
+            __syncwarp();
+            if (lane == 0)
+              for (int32_t k = 0; k < cnt; k++) accw = accw + scratch[k];
+            __syncwarp();
+          }
+          if (lane == 0) epi(r0 + w, w, accw, slices);
+        }
+      } else {
 #pragma unroll
-      for (int q = 0; q < RPT; q++) {
-        const int i = threadIdx.x + q * kThreads;
-        if (i < rows) epi(r0 + i, i, acc[q], slices);
+        for (int q = 0; q < RPT; q++) {
+          const int i = threadIdx.x + q * kThreads;
+          if (i < rows) epi(r0 + i, i, acc[q], slices);
+        }
       }
       // the last warp done with this stage refills it with the tile S further on
       __syncwarp();

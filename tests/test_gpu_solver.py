@@ -169,3 +169,32 @@ def test_config1_random_sparse_lp():
     ref, got = O.solve(P, p), gpu_solve(P, p)
     assert got.status == ref.status == SolveStatus.OPTIMAL
     assert F.relative_gap(got.objective_value, ref.objective_value) <= 1e-5
+
+
+def test_long_rows_take_the_warp_path_and_match_the_oracle():
+    """A row and a column far denser than a tile stage holds (a budget row over
+    every variable, a variable in every row) go through the warp-per-row path;
+    the sums stay in index order, so the solve matches the oracle as any other."""
+    rng = np.random.default_rng(8)
+    n, m = 3000, 2600
+    rows, cols, vals = [], [], []
+    for r in range(m - 1):  # sparse rows, plus column 0 in every row
+        cs = np.unique(np.concatenate([[0], rng.choice(n, 4, replace=False)]))
+        rows += [r] * len(cs)
+        cols += cs.tolist()
+        vals += rng.uniform(0.5, 1.5, len(cs)).tolist()
+    rows += [m - 1] * n  # the dense budget row
+    cols += list(range(n))
+    vals += [1.0] * n
+    from noaidi_b200.prima import SparseMatrix
+    K = SparseMatrix.from_triplets(m, n, rows, cols, vals)
+    x0 = rng.uniform(0.0, 1.0, n)
+    q = K.multiply(x0) - rng.uniform(0.0, 0.5, m)
+    c = rng.uniform(-1.0, 1.0, n)
+    P = LpProblem(c, K, q, 0, np.zeros(n), np.full(n, 2.0))
+    p = PdhgParams(eps_abs=1e-7, eps_rel=1e-7, max_iterations=200_000)
+    ref = O.solve(P, p)
+    for prec in (64, 32):
+        got = gpu_solve(P, p, precision=prec)
+        assert got.status == ref.status == SolveStatus.OPTIMAL
+        assert F.relative_gap(got.objective_value, ref.objective_value) <= (1e-6 if prec == 64 else 1e-4)
