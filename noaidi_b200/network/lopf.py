@@ -17,9 +17,16 @@ with its conventions, since equivalence is judged against PyPSA's output:
 * primary-energy global constraints (<=): per generator, carrier intensity /
   efficiency x the snapshot's generators weighting (:503-559).
 
-Components the dispatch model does not build (storage units, stores,
-transformers, processes, shunts), extendable capacities, committable
-generators and generator set points are refused rather than dropped: a
+* storage units (Lopf.scala:200-240, :336-395; Storage.scala): discharge,
+  charge, state of charge and spill per snapshot; discharge and charge at
+  the bus; the state of charge carried between snapshots through the
+  efficiencies, the standing loss raised to the elapsed hours (the
+  snapshot's stores weighting), inflow and spill, from the previous snapshot,
+  the last one when cyclic, or the initial state; set points pin it.
+
+Components the dispatch model does not build (stores, transformers,
+processes, shunts), extendable capacities, committable generators and
+generator or storage dispatch set points are refused rather than dropped: a
 dropped component leaves a feasible LP for a different network.
 """
 from __future__ import annotations
@@ -36,7 +43,7 @@ from ..prima.types import LpSolution, PdhgParams, SolveStatus
 from .pypsa_csv import Network
 
 HANDLED = {"Bus", "Carrier", "Generator", "Load", "Line", "Link", "GlobalConstraint", "SubNetwork", "LineType",
-           "Shape"}
+           "Shape", "StorageUnit"}
 
 
 class UnsupportedNetwork(ValueError):
@@ -80,7 +87,8 @@ def _reject(network: Network) -> None:
     unhandled = [f"{c} ({len(t)})" for c, t in network.tables.items() if len(t) and c not in HANDLED]
     if unhandled:
         raise UnsupportedNetwork("network contains unmodelled component(s): " + ", ".join(unhandled))
-    for comp, attr in (("Generator", "p_nom_extendable"), ("Link", "p_nom_extendable"), ("Line", "s_nom_extendable")):
+    for comp, attr in (("Generator", "p_nom_extendable"), ("Link", "p_nom_extendable"), ("Line", "s_nom_extendable"),
+                       ("StorageUnit", "p_nom_extendable")):
         tab = network.table(comp)
         for i in tab.ids:
             if bool(tab.value(attr, i)):
@@ -91,8 +99,20 @@ def _reject(network: Network) -> None:
             raise UnsupportedNetwork(f"Generator '{g}' is committable; unit commitment is not a dispatch LP")
     if "p_set" in gens.series and np.isfinite(gens.series["p_set"]).any():
         raise UnsupportedNetwork("a generator has a p_set, which fixes its dispatch; the dispatch model does not")
+    su = network.table("StorageUnit")
+    for attr in ("p_set", "p_dispatch_set", "p_store_set"):  # Storage.reject (Storage.scala:26-39)
+        if (attr in su.series and np.isfinite(su.series[attr]).any()) or any(
+                math.isfinite(float(su.value(attr, i))) for i in su.ids if attr in su.static):
+            raise UnsupportedNetwork(f"a StorageUnit sets {attr}, which pins its dispatch; not built here")
+    for i in su.ids:
+        if not float(su.value("max_hours", i)) > 0.0:
+            raise UnsupportedNetwork(f"StorageUnit '{i}' has max_hours = {su.value('max_hours', i)}, so it can store nothing")
+        for t in range(len(network.snapshots)):
+            loss = su.at("standing_loss", i, t)
+            if not (0.0 <= loss < 1.0):
+                raise UnsupportedNetwork(f"StorageUnit '{i}' has standing_loss = {loss}, not a fraction below 1")
     buses = set(network.table("Bus").ids)
-    for comp, ports in (("Generator", ("bus",)), ("Load", ("bus",)), ("Line", ("bus0", "bus1")),
+    for comp, ports in (("Generator", ("bus",)), ("Load", ("bus",)), ("StorageUnit", ("bus",)), ("Line", ("bus0", "bus1")),
                         ("Link", ("bus0", "bus1"))):
         tab = network.table(comp)
         for i in tab.ids:
@@ -179,6 +199,7 @@ def build(network: Network) -> Model:
     if not buses:
         raise UnsupportedNetwork("network has no buses")
     gens, lines, links, loads = (network.table(c) for c in ("Generator", "Line", "Link", "Load"))
+    units = network.table("StorageUnit")
     columns, bounds, costs = {}, [], []
 
     def declare(component, entity, t, lo, hi, cost):
@@ -199,6 +220,14 @@ def build(network: Network) -> Model:
             pn = float(links.value("p_nom", k))
             lo, hi = pn * links.at("p_min_pu", k, t), pn * links.at("p_max_pu", k, t)
             declare("Link", k, t, min(lo, hi), max(lo, hi), links.at("marginal_cost", k, t) * w)
+        for u in units.ids:  # four non-negative variables per unit (Lopf.scala:200-240)
+            pn = float(units.value("p_nom", u))
+            declare("StorageUnit-p_dispatch", u, t, 0.0, pn * units.at("p_max_pu", u, t),
+                    units.at("marginal_cost", u, t) * w)
+            declare("StorageUnit-p_store", u, t, 0.0, pn * -units.at("p_min_pu", u, t), 0.0)
+            declare("StorageUnit-state_of_charge", u, t, 0.0, pn * float(units.value("max_hours", u)),
+                    units.at("marginal_cost_storage", u, t) * w)
+            declare("StorageUnit-spill", u, t, 0.0, max(0.0, units.at("inflow", u, t)), units.at("spill_cost", u, t) * w)
 
     b = LpBuilder(len(bounds))
     for j, (lo, hi) in enumerate(bounds):
@@ -210,6 +239,10 @@ def build(network: Network) -> Model:
     for t in range(T):
         for bus in buses:
             terms = [(columns[("Generator", g, t)], 1.0) for g in gens.ids if str(gens.value("bus", g)) == bus]
+            for u in units.ids:
+                if str(units.value("bus", u)) == bus:
+                    terms.append((columns[("StorageUnit-p_dispatch", u, t)], 1.0))
+                    terms.append((columns[("StorageUnit-p_store", u, t)], -1.0))
             for comp, tab in (("Line", lines), ("Link", links)):
                 for e in tab.ids:
                     col = columns[(comp, e, t)]
@@ -221,6 +254,28 @@ def build(network: Network) -> Model:
             b.equality_constraint(terms, demand)
             balance_rows[(bus, t)] = row
             row += 1
+
+    # state of charge, the one constraint coupling snapshots (Lopf.scala:336-395)
+    for u in units.ids:
+        cyclic = bool(units.value("cyclic_state_of_charge", u))
+        initial = float(units.value("state_of_charge_initial", u))
+        for t in range(T):
+            eh = network.weighting("stores", t)
+            eff_d, eff_s = units.at("efficiency_dispatch", u, t), units.at("efficiency_store", u, t)
+            if not eff_d > 0.0:
+                raise UnsupportedNetwork(f"StorageUnit '{u}' has efficiency_dispatch = {eff_d} at snapshot {t}")
+            stand = math.pow(1.0 - units.at("standing_loss", u, t), eh)
+            terms = [(columns[("StorageUnit-state_of_charge", u, t)], 1.0),
+                     (columns[("StorageUnit-p_dispatch", u, t)], eh / eff_d),
+                     (columns[("StorageUnit-p_store", u, t)], -eh * eff_s),
+                     (columns[("StorageUnit-spill", u, t)], eh)]
+            prev = t - 1 if t > 0 else (T - 1 if cyclic else None)
+            if prev is not None:
+                terms.append((columns[("StorageUnit-state_of_charge", u, prev)], -stand))
+            b.equality_constraint(terms, eh * units.at("inflow", u, t) + (initial if prev is None else 0.0))
+            target = units.at("state_of_charge_set", u, t)
+            if math.isfinite(target):
+                b.equality_constraint([(columns[("StorageUnit-state_of_charge", u, t)], 1.0)], target)
 
     cycles = cycle_basis(network)
     imp = {(c, e): impedance(network, c, e, cy.carrier) for cy in cycles for c, e, _ in cy.terms}

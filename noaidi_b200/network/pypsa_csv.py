@@ -35,6 +35,10 @@ DEFAULTS = {
     "Line": {"x": 0.0, "r": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "s_nom_extendable": False},
     "Link": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
              "p_nom_extendable": False},
+    "StorageUnit": {"p_nom": 0.0, "p_min_pu": -1.0, "p_max_pu": 1.0, "max_hours": 1.0, "efficiency_store": 1.0,
+                    "efficiency_dispatch": 1.0, "standing_loss": 0.0, "inflow": 0.0, "state_of_charge_initial": 0.0,
+                    "cyclic_state_of_charge": False, "marginal_cost": 0.0, "marginal_cost_storage": 0.0,
+                    "spill_cost": 0.0, "state_of_charge_set": math.nan, "p_nom_extendable": False},
     "GlobalConstraint": {"type": "primary_energy", "carrier_attribute": "co2_emissions", "sense": "=="},
     "Carrier": {"co2_emissions": 0.0},
 }

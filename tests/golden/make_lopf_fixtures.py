@@ -11,11 +11,12 @@ import shutil
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle"]
+NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle"]
 # input tables only: component lists, their input series and the snapshots
 INPUTS = ["buses.csv", "carriers.csv", "generators.csv", "generators-p_max_pu.csv", "generators-p_min_pu.csv",
           "generators-marginal_cost.csv", "lines.csv", "links.csv", "loads.csv", "loads-p_set.csv", "snapshots.csv",
-          "global_constraints.csv"]
+          "global_constraints.csv", "storage_units.csv", "storage_units-inflow.csv",
+          "storage_units-state_of_charge_set.csv"]
 
 
 def main(root):
@@ -29,7 +30,9 @@ def main(root):
                 shutil.copyfile(os.path.join(src, f), os.path.join(dst, f))
         full = json.load(open(os.path.join(goldens, "results", f"{name}.json")))
         res = full["optimize"]
-        keep = {k: res[k] for k in ("objective", "status", "condition", "generator_p", "line_p0", "link_p0")}
+        keep = {k: res[k] for k in ("objective", "status", "condition", "generator_p", "line_p0", "link_p0",
+                                    "storage_p_dispatch", "storage_p_store", "storage_state_of_charge",
+                                    "storage_spill") if k in res}
         if "sclopf" in full:  # the security-constrained solve, with the outages PyPSA used
             keep["sclopf"] = {k: full["sclopf"][k] for k in ("branch_outages", "objective", "status", "generator_p",
                                                              "line_p0")}

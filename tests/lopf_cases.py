@@ -30,7 +30,7 @@ def frame_value(frame, t, column):
     return float("nan") if isinstance(v, dict) else float(v)
 
 
-NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle"]
+NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle"]
 
 
 def check_against_pypsa(solve, name="ac-dc-dispatch"):
@@ -46,7 +46,7 @@ def check_against_pypsa(solve, name="ac-dc-dispatch"):
     # dispatch and flows are compared where the optimum is unique (the
     # reference's LopfSuite does so on ac-dc-dispatch); elsewhere the objective
     # and the ratings are what is determined
-    unique = name == "ac-dc-dispatch"
+    unique = name in ("ac-dc-dispatch", "storage-cycle")
     for t in range(len(n.snapshots)):
         for g in gens.ids if unique else ():
             assert res.dispatch("Generator", g, t) == pytest.approx(frame_value(exp["generator_p"], t, g), abs=1e-3)
@@ -55,7 +55,12 @@ def check_against_pypsa(solve, name="ac-dc-dispatch"):
             assert abs(flow) <= float(lines.value("s_nom", l)) * lines.at("s_max_pu", l, t) + 1e-6
             if unique:
                 assert flow == pytest.approx(frame_value(exp["line_p0"], t, l), abs=1e-3)
-        if not n.table("Link").ids:  # with no links, generation meets load at every snapshot
+        for u in n.table("StorageUnit").ids:  # the storage trajectory (LopfSuite.scala:452-)
+            for comp, key in (("StorageUnit-p_dispatch", "storage_p_dispatch"), ("StorageUnit-p_store", "storage_p_store"),
+                              ("StorageUnit-state_of_charge", "storage_state_of_charge"),
+                              ("StorageUnit-spill", "storage_spill")):
+                assert res.dispatch(comp, u, t) == pytest.approx(frame_value(exp[key], t, u), abs=1e-3), (comp, u, t)
+        if not n.table("Link").ids and not n.table("StorageUnit").ids:  # generation meets load at every snapshot
             generated = sum(res.dispatch("Generator", g, t) for g in gens.ids)
             demanded = sum(loads.at("p_set", d, t) for d in loads.ids)
             assert generated == pytest.approx(demanded, abs=1e-3)

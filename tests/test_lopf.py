@@ -21,7 +21,7 @@ def test_cycle_basis_has_the_circuit_rank():
 def test_unmodelled_components_are_refused():
     from noaidi_b200.network.pypsa_csv import Table
     n = X.network()
-    n.tables["StorageUnit"] = Table("StorageUnit", ["battery"], {"bus": {"battery": "London"}})
+    n.tables["Store"] = Table("Store", ["tank"], {"bus": {"tank": "London"}})
     with pytest.raises(lopf.UnsupportedNetwork):
         lopf.build(n)
 
