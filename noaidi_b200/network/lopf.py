@@ -24,10 +24,17 @@ with its conventions, since equivalence is judged against PyPSA's output:
   snapshot's stores weighting), inflow and spill, from the previous snapshot,
   the last one when cyclic, or the initial state; set points pin it.
 
+* capacity expansion (Expansion.scala; Lopf.scala:124-146, :453-478): one
+  capacity column per extendable entity over the horizon, bounded by
+  ``<nom>_min``/``<nom>_max`` and costed at capital plus fixed O&M cost; the
+  entity's operational columns become unbounded and two rows per snapshot
+  tie them to min_pu and max_pu times the capacity; the objective is the
+  cost of the change, so the existing capacity's cost is subtracted.
+
 Components the dispatch model does not build (stores, transformers,
-processes, shunts), extendable capacities, committable generators and
-generator or storage dispatch set points are refused rather than dropped: a
-dropped component leaves a feasible LP for a different network.
+processes, shunts), committable generators, generator or storage dispatch
+set points, and annuitised or modular capacities are refused rather than
+dropped: a dropped component leaves a feasible LP for a different network.
 """
 from __future__ import annotations
 
@@ -63,6 +70,7 @@ class Model:
     columns: dict      # (component, id, t) -> column
     balance_rows: dict  # (bus, t) -> row of the builder's constraints (before standard form)
     cycles: list
+    objective_constant: float = 0.0  # cost of the capacity the network came with, extendables only
 
 
 @dataclass
@@ -79,20 +87,44 @@ class LopfResult:
     def objective(self) -> float:
         return self.solution.objective_value
 
+    @property
+    def total_system_cost(self) -> float:
+        """PyPSA's objective plus its ``objective_constant``: the cost of the
+        whole optimal capacity rather than of the change."""
+        return self.objective + self.model.objective_constant
+
     def dispatch(self, component: str, entity: str, t: int) -> float:
         return float(self.solution.primal[self.model.columns[(component, entity, t)]])
+
+    def capacity(self, component: str, entity: str) -> float:
+        """The chosen capacity of an extendable entity, else its given one
+        (``LopfResult.capacity``)."""
+        nom = NOMINAL[component]
+        col = self.model.columns.get((f"{component}-{nom}", entity, -1))
+        if col is None:
+            return float(self.network.table(component).value(nom, entity))
+        return float(self.solution.primal[col])
 
 
 def _reject(network: Network) -> None:
     unhandled = [f"{c} ({len(t)})" for c, t in network.tables.items() if len(t) and c not in HANDLED]
     if unhandled:
         raise UnsupportedNetwork("network contains unmodelled component(s): " + ", ".join(unhandled))
-    for comp, attr in (("Generator", "p_nom_extendable"), ("Link", "p_nom_extendable"), ("Line", "s_nom_extendable"),
-                       ("StorageUnit", "p_nom_extendable")):
+    for comp, nom in NOMINAL.items():  # Expansion.reject (Expansion.scala:133-190)
         tab = network.table(comp)
         for i in tab.ids:
-            if bool(tab.value(attr, i)):
-                raise UnsupportedNetwork(f"{comp} '{i}' is extendable; capacity expansion is not in the dispatch model")
+            if not extendable(tab, i):
+                continue
+            if "overnight_cost" in tab.static and math.isfinite(float(tab.value("overnight_cost", i))):
+                raise UnsupportedNetwork(f"{comp} '{i}' sets overnight_cost; only capital_cost is modelled")
+            mod = float(tab.value(f"{nom}_mod", i)) if f"{nom}_mod" in tab.static else math.nan
+            if math.isfinite(mod) and mod > 0.0:
+                raise UnsupportedNetwork(f"{comp} '{i}' sets {nom}_mod: a modular capacity is mixed-integer")
+            lo, hi = float(tab.value(f"{nom}_min", i)), float(tab.value(f"{nom}_max", i))
+            if lo > hi:
+                raise UnsupportedNetwork(f"{comp} '{i}' has {nom}_min = {lo} above {nom}_max = {hi}")
+            if not lo >= 0.0:
+                raise UnsupportedNetwork(f"{comp} '{i}' has {nom}_min = {lo}, which is not a capacity")
     gens = network.table("Generator")
     for g in gens.ids:
         if bool(gens.value("committable", g)) is True:
@@ -119,6 +151,25 @@ def _reject(network: Network) -> None:
             for port in ports:
                 if str(tab.value(port, i)) not in buses:
                     raise UnsupportedNetwork(f"{comp} '{i}' references unknown bus '{tab.value(port, i)}' via {port}")
+
+
+NOMINAL = {"Generator": "p_nom", "Line": "s_nom", "Link": "p_nom", "StorageUnit": "p_nom"}
+
+
+def extendable(tab, entity: str) -> bool:
+    """``Expansion.isExtendable``: the ``<nom>_extendable`` flag."""
+    nom = NOMINAL.get(tab.component)
+    return nom is not None and f"{nom}_extendable" in tab.static and bool(tab.value(f"{nom}_extendable", entity))
+
+
+def periodized_cost(tab, entity: str) -> float:
+    """``Expansion.periodizedCost``: capital cost plus fixed O&M cost."""
+    total = 0.0
+    for attr in ("capital_cost", "fom_cost"):
+        v = float(tab.value(attr, entity))
+        if math.isfinite(v):
+            total += v
+    return total
 
 
 def cycle_basis(network: Network) -> list:
@@ -207,25 +258,46 @@ def build(network: Network) -> Model:
         bounds.append((lo, hi))
         costs.append(cost)
 
+    # capacity columns first, one per extendable entity over the horizon
+    expandable = [(c, network.table(c), [i for i in network.table(c).ids if extendable(network.table(c), i)])
+                  for c in ("Line", "Link", "Generator", "StorageUnit")]
+    expandable = [(c, tab, ids) for c, tab, ids in expandable if ids]
+    for c, tab, ids in expandable:
+        nom = NOMINAL[c]
+        for i in ids:
+            declare(f"{c}-{nom}", i, -1, float(tab.value(f"{nom}_min", i)), float(tab.value(f"{nom}_max", i)),
+                    periodized_cost(tab, i))
+
     for t in range(T):
         w = network.weighting("objective", t)
         for g in gens.ids:
+            if extendable(gens, g):
+                declare("Generator", g, t, -math.inf, math.inf, gens.at("marginal_cost", g, t) * w)
+                continue
             pn = float(gens.value("p_nom", g))
             lo, hi = pn * gens.at("p_min_pu", g, t), pn * gens.at("p_max_pu", g, t)
             declare("Generator", g, t, min(lo, hi), max(lo, hi), gens.at("marginal_cost", g, t) * w)
         for l in lines.ids:
+            if extendable(lines, l):
+                declare("Line", l, t, -math.inf, math.inf, 0.0)
+                continue
             lim = float(lines.value("s_nom", l)) * lines.at("s_max_pu", l, t)
             declare("Line", l, t, -lim, lim, 0.0)
         for k in links.ids:
+            if extendable(links, k):
+                declare("Link", k, t, -math.inf, math.inf, links.at("marginal_cost", k, t) * w)
+                continue
             pn = float(links.value("p_nom", k))
             lo, hi = pn * links.at("p_min_pu", k, t), pn * links.at("p_max_pu", k, t)
             declare("Link", k, t, min(lo, hi), max(lo, hi), links.at("marginal_cost", k, t) * w)
         for u in units.ids:  # four non-negative variables per unit (Lopf.scala:200-240)
             pn = float(units.value("p_nom", u))
-            declare("StorageUnit-p_dispatch", u, t, 0.0, pn * units.at("p_max_pu", u, t),
+            ext = extendable(units, u)
+            upper = (lambda v: math.inf) if ext else (lambda v: pn * v)
+            declare("StorageUnit-p_dispatch", u, t, 0.0, upper(units.at("p_max_pu", u, t)),
                     units.at("marginal_cost", u, t) * w)
-            declare("StorageUnit-p_store", u, t, 0.0, pn * -units.at("p_min_pu", u, t), 0.0)
-            declare("StorageUnit-state_of_charge", u, t, 0.0, pn * float(units.value("max_hours", u)),
+            declare("StorageUnit-p_store", u, t, 0.0, upper(-units.at("p_min_pu", u, t)), 0.0)
+            declare("StorageUnit-state_of_charge", u, t, 0.0, upper(float(units.value("max_hours", u))),
                     units.at("marginal_cost_storage", u, t) * w)
             declare("StorageUnit-spill", u, t, 0.0, max(0.0, units.at("inflow", u, t)), units.at("spill_cost", u, t) * w)
 
@@ -234,6 +306,8 @@ def build(network: Network) -> Model:
         b.bounds(j, lo, hi)
     for j, c in enumerate(costs):
         b.objective_coefficient(j, c)
+    constant = sum(periodized_cost(tab, i) * float(tab.value(NOMINAL[c], i)) for c, tab, ids in expandable for i in ids)
+    b.objective_offset(-constant)  # PyPSA reports the cost of the change (Lopf.scala:255-262)
 
     balance_rows, row = {}, 0
     for t in range(T):
@@ -287,6 +361,28 @@ def build(network: Network) -> Model:
         for cy in cycles:
             b.equality_constraint([(columns[(c, e, t)], o * imp[(c, e)]) for c, e, o in cy.terms], 0.0)
 
+    # capacity coupling, after every equality block (Lopf.scala:453-478)
+    for c, tab, ids in expandable:
+        nom = NOMINAL[c]
+        for i in ids:
+            cap = columns[(f"{c}-{nom}", i, -1)]
+            for t in range(T):
+                if c == "Line":
+                    mx = tab.at("s_max_pu", i, t)
+                    pairs = [("Line", -mx, mx)]
+                elif c == "StorageUnit":
+                    pairs = [("StorageUnit-p_dispatch", -math.inf, tab.at("p_max_pu", i, t)),
+                             ("StorageUnit-p_store", -math.inf, -tab.at("p_min_pu", i, t)),
+                             ("StorageUnit-state_of_charge", -math.inf, float(tab.value("max_hours", i)))]
+                else:
+                    pairs = [(c, tab.at("p_min_pu", i, t), tab.at("p_max_pu", i, t))]
+                for var, min_pu, max_pu in pairs:
+                    col = columns[(var, i, t)]
+                    if math.isfinite(max_pu):
+                        b.less_than([(col, 1.0), (cap, -max_pu)], 0.0)
+                    if math.isfinite(min_pu):
+                        b.greater_than([(col, 1.0), (cap, -min_pu)], 0.0)
+
     constraints = network.table("GlobalConstraint")
     carriers = network.table("Carrier")
     for gc in constraints.ids:
@@ -311,7 +407,7 @@ def build(network: Network) -> Model:
             b.less_than(terms, float(constraints.value("constant", gc)))
 
     problem, translation = b.build()
-    return Model(problem, translation, columns, balance_rows, cycles)
+    return Model(problem, translation, columns, balance_rows, cycles, constant)
 
 
 def solve(network: Network, params: PdhgParams = PdhgParams(), precision: int = 64, device: int = 0,
@@ -455,4 +551,4 @@ def build_sclopf(network: Network, outages: Optional[list] = None) -> Model:
                     if factor != 0.0:
                         b.constraint([(col, 1.0), (base.columns[("Line", o, t)], factor)], -limit, limit)
     problem, translation = b.build()
-    return Model(problem, translation, base.columns, base.balance_rows, base.cycles)
+    return Model(problem, translation, base.columns, base.balance_rows, base.cycles, base.objective_constant)

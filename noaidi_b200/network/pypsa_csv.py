@@ -30,15 +30,18 @@ LIST_NAMES = {
 DEFAULTS = {
     "Bus": {"v_nom": 1.0, "carrier": "AC"},
     "Generator": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
-                  "p_nom_extendable": False, "committable": False, "carrier": ""},
+                  "p_nom_extendable": False, "committable": False, "carrier": "", "p_nom_min": 0.0,
+                  "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
     "Load": {"p_set": 0.0},
-    "Line": {"x": 0.0, "r": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "s_nom_extendable": False},
+    "Line": {"x": 0.0, "r": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "s_nom_extendable": False, "s_nom_min": 0.0,
+             "s_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
     "Link": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
-             "p_nom_extendable": False},
+             "p_nom_extendable": False, "p_nom_min": 0.0, "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
     "StorageUnit": {"p_nom": 0.0, "p_min_pu": -1.0, "p_max_pu": 1.0, "max_hours": 1.0, "efficiency_store": 1.0,
                     "efficiency_dispatch": 1.0, "standing_loss": 0.0, "inflow": 0.0, "state_of_charge_initial": 0.0,
                     "cyclic_state_of_charge": False, "marginal_cost": 0.0, "marginal_cost_storage": 0.0,
-                    "spill_cost": 0.0, "state_of_charge_set": math.nan, "p_nom_extendable": False},
+                    "spill_cost": 0.0, "state_of_charge_set": math.nan, "p_nom_extendable": False,
+                    "p_nom_min": 0.0, "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
     "GlobalConstraint": {"type": "primary_energy", "carrier_attribute": "co2_emissions", "sense": "=="},
     "Carrier": {"co2_emissions": 0.0},
 }
@@ -88,14 +91,28 @@ class Network:
         return 1.0 if w is None else float(w[t])
 
 
-def _coerce(v):
+# Attributes that name other entities or labels: kept as text even when they
+# read as numbers (bus "0" is a name, not a zero).
+LABELS = frozenset({"bus", "bus0", "bus1", "bus2", "bus3", "carrier", "control", "type", "sub_network",
+                    "generator", "country", "location", "unit", "sense", "investment_period"})
+
+
+def _coerce(v, label: bool = False):
+    if v is None or (isinstance(v, float) and math.isnan(v)):
+        return math.nan
+    if label:
+        return str(v)
+    if isinstance(v, str):
+        t = v.strip()
+        if t.lower() in ("true", "false"):
+            return t.lower() == "true"
+        try:
+            return float(t)
+        except ValueError:
+            return v
     if isinstance(v, (bool, np.bool_)):
         return bool(v)
-    if isinstance(v, (int, float, np.integer, np.floating)):
-        return float(v)
-    if isinstance(v, str) and v.lower() in ("true", "false"):
-        return v.lower() == "true"
-    return v
+    return float(v)
 
 
 def read(folder: str, name: str = "") -> Network:
@@ -109,11 +126,11 @@ def read(folder: str, name: str = "") -> Network:
     for component, stem in LIST_NAMES.items():
         if f"{stem}.csv" not in files:
             continue
-        df = pd.read_csv(os.path.join(folder, f"{stem}.csv"), keep_default_na=True)
+        df = pd.read_csv(os.path.join(folder, f"{stem}.csv"), dtype=str, keep_default_na=True)
         if df.empty:
             continue
         ids = [str(v) for v in df[df.columns[0]]]
-        static = {col: {i: _coerce(v) for i, v in zip(ids, df[col])} for col in df.columns[1:]}
+        static = {col: {i: _coerce(v, col in LABELS) for i, v in zip(ids, df[col])} for col in df.columns[1:]}
         series = {}
         for f in files:
             if f.startswith(stem + "-") and f.endswith(".csv"):

@@ -1,5 +1,6 @@
 """Copies the input tables of PyPSA golden networks and the expected LOPF
-results (objective, generator dispatch, line flows) from the reference's
+results (objective, generator dispatch, line flows, storage trajectories,
+optimal capacities and the objective constant) from the reference's
 goldens (reference/goldens/{networks,results} in oluies/noaidi, generated by
 PyPSA 1.2.4) into tests/golden/lopf/<network>/.
 
@@ -11,7 +12,7 @@ import shutil
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle"]
+NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle", "ac-dc-meshed", "storage-hvdc"]
 # input tables only: component lists, their input series and the snapshots
 INPUTS = ["buses.csv", "carriers.csv", "generators.csv", "generators-p_max_pu.csv", "generators-p_min_pu.csv",
           "generators-marginal_cost.csv", "lines.csv", "links.csv", "loads.csv", "loads-p_set.csv", "snapshots.csv",
@@ -32,7 +33,8 @@ def main(root):
         res = full["optimize"]
         keep = {k: res[k] for k in ("objective", "status", "condition", "generator_p", "line_p0", "link_p0",
                                     "storage_p_dispatch", "storage_p_store", "storage_state_of_charge",
-                                    "storage_spill") if k in res}
+                                    "storage_spill", "objective_constant", "total_system_cost", "nominal_opt")
+                if k in res}
         if "sclopf" in full:  # the security-constrained solve, with the outages PyPSA used
             keep["sclopf"] = {k: full["sclopf"][k] for k in ("branch_outages", "objective", "status", "generator_p",
                                                              "line_p0")}

@@ -30,7 +30,8 @@ def frame_value(frame, t, column):
     return float("nan") if isinstance(v, dict) else float(v)
 
 
-NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle"]
+NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle", "ac-dc-meshed",
+            "storage-hvdc"]
 
 
 def check_against_pypsa(solve, name="ac-dc-dispatch"):
@@ -52,10 +53,10 @@ def check_against_pypsa(solve, name="ac-dc-dispatch"):
             assert res.dispatch("Generator", g, t) == pytest.approx(frame_value(exp["generator_p"], t, g), abs=1e-3)
         for l in lines.ids:
             flow = res.dispatch("Line", l, t)
-            assert abs(flow) <= float(lines.value("s_nom", l)) * lines.at("s_max_pu", l, t) + 1e-6
+            assert abs(flow) <= res.capacity("Line", l) * lines.at("s_max_pu", l, t) + 1e-6
             if unique:
                 assert flow == pytest.approx(frame_value(exp["line_p0"], t, l), abs=1e-3)
-        for u in n.table("StorageUnit").ids:  # the storage trajectory (LopfSuite.scala:452-)
+        for u in n.table("StorageUnit").ids if unique else ():  # the storage trajectory (LopfSuite.scala:452-)
             for comp, key in (("StorageUnit-p_dispatch", "storage_p_dispatch"), ("StorageUnit-p_store", "storage_p_store"),
                               ("StorageUnit-state_of_charge", "storage_state_of_charge"),
                               ("StorageUnit-spill", "storage_spill")):
@@ -64,6 +65,24 @@ def check_against_pypsa(solve, name="ac-dc-dispatch"):
             generated = sum(res.dispatch("Generator", g, t) for g in gens.ids)
             demanded = sum(loads.at("p_set", d, t) for d in loads.ids)
             assert generated == pytest.approx(demanded, abs=1e-3)
+    if "nominal_opt" in exp:  # expansion: the capacities are the answer (LopfSuite.scala:258-318)
+        constant = exp.get("objective_constant", 0.0)
+        assert res.total_system_cost - res.objective == pytest.approx(constant, abs=1e-6 * max(1.0, abs(constant)))
+        total = exp["total_system_cost"]
+        assert res.total_system_cost == pytest.approx(total, abs=1e-6 * max(1.0, abs(total)))
+        compared = moved = 0
+        for component, chosen in exp["nominal_opt"].items():
+            tab = n.table(component)
+            for i, value in chosen.items():
+                if i not in tab.ids:
+                    continue
+                got = res.capacity(component, i)
+                assert got == pytest.approx(value, abs=1e-4 * max(1.0, abs(value))), (component, i)
+                compared += 1
+                moved += abs(value - float(tab.value(lopf.NOMINAL[component], i))) > 1.0
+        assert compared > 0
+        if constant != 0.0:  # an expansion network: many capacities chosen, some moved
+            assert compared > 10 and moved, (compared, moved)
     return res
 
 

@@ -53,3 +53,46 @@ def test_a_bridge_is_not_a_credible_contingency():
     bus.static.setdefault("v_nom", {})["D"] = 380.0
     with pytest.raises(lopf.UnsupportedNetwork):
         lopf.build_sclopf(n, ["spur"])
+
+
+def _with_generator_attr(attr, value):
+    n = X.network("ac-dc-meshed")
+    gens = n.table("Generator")
+    gens.static[attr] = {g: value for g in gens.ids}
+    return n
+
+
+@pytest.mark.parametrize("attr,value,word", [
+    ("overnight_cost", 1000.0, "overnight_cost"),  # annuitised cost is not a per-unit one (LopfSuite.scala:222-238)
+    ("p_nom_mod", 100.0, "p_nom_mod"),             # modular capacity is mixed-integer (:240-255)
+    ("p_nom_min", -5.0, "p_nom_min"),              # a negative capacity floor
+])
+def test_expansion_attributes_the_lp_cannot_honour_are_refused(attr, value, word):
+    with pytest.raises(lopf.UnsupportedNetwork, match=word):
+        lopf.build(_with_generator_attr(attr, value))
+
+
+def test_expansion_bounds_that_cross_are_refused():
+    n = X.network("ac-dc-meshed")
+    gens = n.table("Generator")
+    g = next(i for i in gens.ids if lopf.extendable(gens, i))
+    gens.static.setdefault("p_nom_min", {})[g] = 10.0
+    gens.static.setdefault("p_nom_max", {})[g] = 5.0
+    with pytest.raises(lopf.UnsupportedNetwork, match="above"):
+        lopf.build(n)
+
+
+def test_a_non_extendable_network_builds_no_capacity_columns():
+    model = lopf.build(X.network("ac-dc-dispatch"))
+    assert not [k for k in model.columns if k[2] == -1]
+    assert model.objective_constant == 0.0
+
+
+def test_capacity_columns_come_first_and_carry_capital_cost():
+    n = X.network("ac-dc-meshed")
+    model = lopf.build(n)
+    caps = sorted((col, k) for k, col in model.columns.items() if k[2] == -1)
+    assert [c for c, _ in caps] == list(range(len(caps)))  # declared before every snapshot column
+    for col, (component, entity, _) in caps:
+        tab = n.table(component.split("-")[0])
+        assert model.problem.objective[col] == pytest.approx(lopf.periodized_cost(tab, entity))
