@@ -24,6 +24,11 @@ with its conventions, since equivalence is judged against PyPSA's output:
   snapshot's stores weighting), inflow and spill, from the previous snapshot,
   the last one when cyclic, or the initial state; set points pin it.
 
+* stores (Stores.scala; Lopf.scala:242-265, :440-467): an energy level in
+  e_nom x [e_min_pu, e_max_pu] and one signed power with no rating, positive
+  into the bus; e(t) = (1 - standing_loss)^eh e(t-1) - eh p(t), wrapping to
+  the last snapshot when cyclic, else starting from e_initial.
+
 * capacity expansion (Expansion.scala; Lopf.scala:124-146, :453-478): one
   capacity column per extendable entity over the horizon, bounded by
   ``<nom>_min``/``<nom>_max`` and costed at capital plus fixed O&M cost; the
@@ -31,9 +36,9 @@ with its conventions, since equivalence is judged against PyPSA's output:
   tie them to min_pu and max_pu times the capacity; the objective is the
   cost of the change, so the existing capacity's cost is subtracted.
 
-Components the dispatch model does not build (stores, transformers,
-processes, shunts), committable generators, generator or storage dispatch
-set points, and annuitised or modular capacities are refused rather than
+Components the dispatch model does not build (transformers, processes,
+shunts), committable generators, generator, storage or store set points, and
+annuitised or modular capacities are refused rather than
 dropped: a dropped component leaves a feasible LP for a different network.
 """
 from __future__ import annotations
@@ -50,7 +55,7 @@ from ..prima.types import LpSolution, PdhgParams, SolveStatus
 from .pypsa_csv import Network
 
 HANDLED = {"Bus", "Carrier", "Generator", "Load", "Line", "Link", "GlobalConstraint", "SubNetwork", "LineType",
-           "Shape", "StorageUnit"}
+           "Shape", "StorageUnit", "Store"}
 
 
 class UnsupportedNetwork(ValueError):
@@ -139,10 +144,22 @@ def _reject(network: Network) -> None:
     for i in su.ids:
         if not float(su.value("max_hours", i)) > 0.0:
             raise UnsupportedNetwork(f"StorageUnit '{i}' has max_hours = {su.value('max_hours', i)}, so it can store nothing")
-        for t in range(len(network.snapshots)):
-            loss = su.at("standing_loss", i, t)
-            if not (0.0 <= loss < 1.0):
-                raise UnsupportedNetwork(f"StorageUnit '{i}' has standing_loss = {loss}, not a fraction below 1")
+    _reject_standing_loss(network, su)
+    st = network.table("Store")
+    for attr, what in (("e_set", "its energy"), ("p_set", "its power")):  # Stores.reject (Stores.scala:48-90)
+        pinned = [i for i in st.ids if attr in st.static and math.isfinite(float(st.value(attr, i)))]
+        if attr in st.series and np.isfinite(st.series[attr]).any():
+            pinned.append("(series)")
+        if pinned:
+            raise UnsupportedNetwork(f"Store '{pinned[0]}' sets {attr}, which pins {what}; that constraint is "
+                                     "not built here")
+    for attr in ("e_cyclic_per_period", "e_initial_per_period"):
+        if any(attr in st.static and bool(st.value(attr, i)) is True for i in st.ids):
+            raise UnsupportedNetwork(f"a Store sets {attr}, a multi-period concept; this model has one horizon")
+    if any(float(st.value("marginal_cost_quadratic", i)) != 0.0 for i in st.ids) or \
+            ("marginal_cost_quadratic" in st.series and np.any(st.series["marginal_cost_quadratic"] != 0.0)):
+        raise UnsupportedNetwork("a Store has a non-zero marginal_cost_quadratic; the objective here is linear")
+    _reject_standing_loss(network, st)
     buses = set(network.table("Bus").ids)
     for comp, ports in (("Generator", ("bus",)), ("Load", ("bus",)), ("StorageUnit", ("bus",)), ("Line", ("bus0", "bus1")),
                         ("Link", ("bus0", "bus1"))):
@@ -153,7 +170,8 @@ def _reject(network: Network) -> None:
                     raise UnsupportedNetwork(f"{comp} '{i}' references unknown bus '{tab.value(port, i)}' via {port}")
 
 
-NOMINAL = {"Generator": "p_nom", "Line": "s_nom", "Link": "p_nom", "StorageUnit": "p_nom"}
+NOMINAL = {"Generator": "p_nom", "Line": "s_nom", "Link": "p_nom", "StorageUnit": "p_nom", "Store": "e_nom"}
+EXPANSION_ORDER = ("Line", "Link", "Generator", "StorageUnit", "Store")
 
 
 def extendable(tab, entity: str) -> bool:
@@ -170,6 +188,17 @@ def periodized_cost(tab, entity: str) -> float:
         if math.isfinite(v):
             total += v
     return total
+
+
+def _reject_standing_loss(network: Network, tab) -> None:
+    """``Losses.rejectStandingLoss``: a standing loss outside [0, 1) at any
+    snapshot the energy balance reads is a gain, not a loss."""
+    for i in tab.ids:
+        for t in range(len(network.snapshots)):
+            loss = tab.at("standing_loss", i, t)
+            if not (0.0 <= loss < 1.0):
+                raise UnsupportedNetwork(f"{tab.component} '{i}' has standing_loss = {loss} at snapshot {t}, "
+                                         "not a fraction below 1")
 
 
 def cycle_basis(network: Network) -> list:
@@ -250,7 +279,7 @@ def build(network: Network) -> Model:
     if not buses:
         raise UnsupportedNetwork("network has no buses")
     gens, lines, links, loads = (network.table(c) for c in ("Generator", "Line", "Link", "Load"))
-    units = network.table("StorageUnit")
+    units, stores = network.table("StorageUnit"), network.table("Store")
     columns, bounds, costs = {}, [], []
 
     def declare(component, entity, t, lo, hi, cost):
@@ -260,7 +289,7 @@ def build(network: Network) -> Model:
 
     # capacity columns first, one per extendable entity over the horizon
     expandable = [(c, network.table(c), [i for i in network.table(c).ids if extendable(network.table(c), i)])
-                  for c in ("Line", "Link", "Generator", "StorageUnit")]
+                  for c in EXPANSION_ORDER]
     expandable = [(c, tab, ids) for c, tab, ids in expandable if ids]
     for c, tab, ids in expandable:
         nom = NOMINAL[c]
@@ -300,6 +329,14 @@ def build(network: Network) -> Model:
             declare("StorageUnit-state_of_charge", u, t, 0.0, upper(float(units.value("max_hours", u))),
                     units.at("marginal_cost_storage", u, t) * w)
             declare("StorageUnit-spill", u, t, 0.0, max(0.0, units.at("inflow", u, t)), units.at("spill_cost", u, t) * w)
+        for s_ in stores.ids:  # energy and one signed, unrated power (Lopf.scala:242-265)
+            if extendable(stores, s_):
+                lo, hi = -math.inf, math.inf
+            else:
+                e_nom = float(stores.value("e_nom", s_))
+                lo, hi = e_nom * stores.at("e_min_pu", s_, t), e_nom * stores.at("e_max_pu", s_, t)
+            declare("Store-e", s_, t, min(lo, hi), max(lo, hi), stores.at("marginal_cost_storage", s_, t) * w)
+            declare("Store-p", s_, t, -math.inf, math.inf, stores.at("marginal_cost", s_, t) * w)
 
     b = LpBuilder(len(bounds))
     for j, (lo, hi) in enumerate(bounds):
@@ -317,6 +354,7 @@ def build(network: Network) -> Model:
                 if str(units.value("bus", u)) == bus:
                     terms.append((columns[("StorageUnit-p_dispatch", u, t)], 1.0))
                     terms.append((columns[("StorageUnit-p_store", u, t)], -1.0))
+            terms += [(columns[("Store-p", s_, t)], 1.0) for s_ in stores.ids if str(stores.value("bus", s_)) == bus]
             for comp, tab in (("Line", lines), ("Link", links)):
                 for e in tab.ids:
                     col = columns[(comp, e, t)]
@@ -361,6 +399,19 @@ def build(network: Network) -> Model:
         for cy in cycles:
             b.equality_constraint([(columns[(c, e, t)], o * imp[(c, e)]) for c, e, o in cy.terms], 0.0)
 
+    # a store's energy: e(t) = (1 - standing_loss)^eh e(t-1) - eh p(t) (Lopf.scala:440-467)
+    for s_ in stores.ids:
+        cyclic = bool(stores.value("e_cyclic", s_)) is True
+        initial = float(stores.value("e_initial", s_))
+        for t in range(T):
+            eh = network.weighting("stores", t)
+            stand = math.pow(1.0 - stores.at("standing_loss", s_, t), eh)
+            terms = [(columns[("Store-e", s_, t)], 1.0), (columns[("Store-p", s_, t)], eh)]
+            prev = t - 1 if t > 0 else (T - 1 if cyclic else None)
+            if prev is not None:
+                terms.append((columns[("Store-e", s_, prev)], -stand))
+            b.equality_constraint(terms, initial if prev is None else 0.0)
+
     # capacity coupling, after every equality block (Lopf.scala:453-478)
     for c, tab, ids in expandable:
         nom = NOMINAL[c]
@@ -374,6 +425,8 @@ def build(network: Network) -> Model:
                     pairs = [("StorageUnit-p_dispatch", -math.inf, tab.at("p_max_pu", i, t)),
                              ("StorageUnit-p_store", -math.inf, -tab.at("p_min_pu", i, t)),
                              ("StorageUnit-state_of_charge", -math.inf, float(tab.value("max_hours", i)))]
+                elif c == "Store":
+                    pairs = [("Store-e", tab.at("e_min_pu", i, t), tab.at("e_max_pu", i, t))]
                 else:
                     pairs = [(c, tab.at("p_min_pu", i, t), tab.at("p_max_pu", i, t))]
                 for var, min_pu, max_pu in pairs:

@@ -42,6 +42,10 @@ DEFAULTS = {
                     "cyclic_state_of_charge": False, "marginal_cost": 0.0, "marginal_cost_storage": 0.0,
                     "spill_cost": 0.0, "state_of_charge_set": math.nan, "p_nom_extendable": False,
                     "p_nom_min": 0.0, "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
+    "Store": {"e_nom": 0.0, "e_min_pu": 0.0, "e_max_pu": 1.0, "e_initial": 0.0, "e_cyclic": False,
+              "standing_loss": 0.0, "marginal_cost": 0.0, "marginal_cost_storage": 0.0, "marginal_cost_quadratic": 0.0,
+              "p_set": math.nan, "e_set": math.nan, "e_nom_extendable": False, "e_nom_min": 0.0, "e_nom_max": math.inf,
+              "capital_cost": 0.0, "fom_cost": 0.0},
     "GlobalConstraint": {"type": "primary_energy", "carrier_attribute": "co2_emissions", "sense": "=="},
     "Carrier": {"co2_emissions": 0.0},
 }

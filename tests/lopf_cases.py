@@ -31,7 +31,7 @@ def frame_value(frame, t, column):
 
 
 NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle", "ac-dc-meshed",
-            "storage-hvdc"]
+            "storage-hvdc", "store-bank"]
 
 
 def check_against_pypsa(solve, name="ac-dc-dispatch"):
@@ -61,7 +61,10 @@ def check_against_pypsa(solve, name="ac-dc-dispatch"):
                               ("StorageUnit-state_of_charge", "storage_state_of_charge"),
                               ("StorageUnit-spill", "storage_spill")):
                 assert res.dispatch(comp, u, t) == pytest.approx(frame_value(exp[key], t, u), abs=1e-3), (comp, u, t)
-        if not n.table("Link").ids and not n.table("StorageUnit").ids:  # generation meets load at every snapshot
+        for st in n.table("Store").ids:  # energy and signed power (LopfSuite.scala:325-364)
+            assert res.dispatch("Store-e", st, t) == pytest.approx(frame_value(exp["store_e"], t, st), abs=1e-4)
+            assert res.dispatch("Store-p", st, t) == pytest.approx(frame_value(exp["store_p"], t, st), abs=1e-4)
+        if not n.table("Link").ids and not n.table("StorageUnit").ids and not n.table("Store").ids:  # generation meets load at every snapshot
             generated = sum(res.dispatch("Generator", g, t) for g in gens.ids)
             demanded = sum(loads.at("p_set", d, t) for d in loads.ids)
             assert generated == pytest.approx(demanded, abs=1e-3)

@@ -21,7 +21,7 @@ def test_cycle_basis_has_the_circuit_rank():
 def test_unmodelled_components_are_refused():
     from noaidi_b200.network.pypsa_csv import Table
     n = X.network()
-    n.tables["Store"] = Table("Store", ["tank"], {"bus": {"tank": "London"}})
+    n.tables["ShuntImpedance"] = Table("ShuntImpedance", ["shunt"], {"bus": {"shunt": "London"}})
     with pytest.raises(lopf.UnsupportedNetwork):
         lopf.build(n)
 
@@ -96,3 +96,36 @@ def test_capacity_columns_come_first_and_carry_capital_cost():
     for col, (component, entity, _) in caps:
         tab = n.table(component.split("-")[0])
         assert model.problem.objective[col] == pytest.approx(lopf.periodized_cost(tab, entity))
+
+
+def test_a_store_has_no_power_rating():
+    """PyPSA bounds no Store-p: a store's rate follows from its energy band
+    and the elapsed hours alone (LopfSuite.scala:392-414)."""
+    n = X.network("store-bank")
+    model = lopf.build(n)
+    for st in n.table("Store").ids:
+        for t in range(len(n.snapshots)):
+            j = model.columns[("Store-p", st, t)]
+            assert model.problem.variable_lower[j] == -np.inf and model.problem.variable_upper[j] == np.inf
+
+
+def test_the_store_fixture_exercises_its_features():
+    """The cyclic wrap, both ends of the energy band and the capacity ceiling
+    are all binding in PyPSA's answer (LopfSuite.scala:366-390)."""
+    exp = X.expected("store-bank")
+    last = len(X.network("store-bank").snapshots) - 1
+    assert X.frame_value(exp["store_e"], last, "swing") > 1.0
+    assert X.frame_value(exp["store_p"], 0, "swing") > 1.0
+    levels = [X.frame_value(exp["store_e"], t, "tank") for t in range(last + 1)]
+    assert min(levels) == pytest.approx(20.0, abs=1e-3) and max(levels) == pytest.approx(100.0, abs=1e-3)
+    assert exp["nominal_opt"]["Store"]["grow"] == pytest.approx(60.0, abs=1e-3)
+
+
+@pytest.mark.parametrize("attr,value", [("e_set", 50.0), ("p_set", 1.0), ("marginal_cost_quadratic", 0.5),
+                                        ("standing_loss", 1.5), ("e_cyclic_per_period", True)])
+def test_store_features_not_built_are_refused(attr, value):
+    n = X.network("store-bank")
+    st = n.table("Store")
+    st.static[attr] = {i: value for i in st.ids}
+    with pytest.raises(lopf.UnsupportedNetwork):
+        lopf.build(n)
