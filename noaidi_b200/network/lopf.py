@@ -36,8 +36,13 @@ with its conventions, since equivalence is judged against PyPSA's output:
   tie them to min_pu and max_pu times the capacity; the objective is the
   cost of the change, so the existing capacity's cost is subtracted.
 
-Components the dispatch model does not build (transformers, processes,
-shunts), committable generators, generator, storage or store set points, and
+* transformers: passive branches like lines, rated by s_nom x s_max_pu and
+  referred to their own base in Kirchhoff rows, z tap_ratio / s_nom
+  (Cycles.scala:154-193); the phase shift moves angles, not the optimised
+  flows, and is not read.  The security-constrained model monitors and
+  outages lines and transformers alike.
+
+Components the dispatch model does not build (processes, shunts), committable generators, generator, storage or store set points, and
 annuitised or modular capacities are refused rather than
 dropped: a dropped component leaves a feasible LP for a different network.
 """
@@ -54,8 +59,9 @@ from ..prima.model import LpBuilder, LpProblem, Negated, RowTranslation
 from ..prima.types import LpSolution, PdhgParams, SolveStatus
 from .pypsa_csv import Network
 
-HANDLED = {"Bus", "Carrier", "Generator", "Load", "Line", "Link", "GlobalConstraint", "SubNetwork", "LineType",
-           "Shape", "StorageUnit", "Store"}
+HANDLED = {"Bus", "Carrier", "Generator", "Load", "Line", "Transformer", "Link", "GlobalConstraint", "SubNetwork",
+           "LineType", "TransformerType", "Shape", "StorageUnit", "Store"}
+PASSIVE = ("Line", "Transformer")  # branches whose flow follows from impedance
 
 
 class UnsupportedNetwork(ValueError):
@@ -161,7 +167,8 @@ def _reject(network: Network) -> None:
         raise UnsupportedNetwork("a Store has a non-zero marginal_cost_quadratic; the objective here is linear")
     _reject_standing_loss(network, st)
     buses = set(network.table("Bus").ids)
-    for comp, ports in (("Generator", ("bus",)), ("Load", ("bus",)), ("StorageUnit", ("bus",)), ("Line", ("bus0", "bus1")),
+    for comp, ports in (("Generator", ("bus",)), ("Load", ("bus",)), ("StorageUnit", ("bus",)), ("Store", ("bus",)),
+                        ("Line", ("bus0", "bus1")), ("Transformer", ("bus0", "bus1")),
                         ("Link", ("bus0", "bus1"))):
         tab = network.table(comp)
         for i in tab.ids:
@@ -170,8 +177,18 @@ def _reject(network: Network) -> None:
                     raise UnsupportedNetwork(f"{comp} '{i}' references unknown bus '{tab.value(port, i)}' via {port}")
 
 
-NOMINAL = {"Generator": "p_nom", "Line": "s_nom", "Link": "p_nom", "StorageUnit": "p_nom", "Store": "e_nom"}
-EXPANSION_ORDER = ("Line", "Link", "Generator", "StorageUnit", "Store")
+NOMINAL = {"Generator": "p_nom", "Line": "s_nom", "Transformer": "s_nom", "Link": "p_nom", "StorageUnit": "p_nom",
+           "Store": "e_nom"}
+EXPANSION_ORDER = ("Line", "Transformer", "Link", "Generator", "StorageUnit", "Store")
+
+
+def passive_branches(network: Network) -> list:
+    """(component, id, bus0, bus1) of every line and transformer, lines first."""
+    out = []
+    for c in PASSIVE:
+        tab = network.table(c)
+        out += [(c, i, str(tab.value("bus0", i)), str(tab.value("bus1", i))) for i in tab.ids]
+    return out
 
 
 def extendable(tab, entity: str) -> bool:
@@ -206,8 +223,7 @@ def cycle_basis(network: Network) -> list:
     breadth-first spanning tree and one cycle per non-tree edge (circuit rank
     edges - nodes + components).  orientation +1 where the cycle runs bus0 to
     bus1.  Any basis spans the same constraints."""
-    lines = network.table("Line")
-    edges = [("Line", i, str(lines.value("bus0", i)), str(lines.value("bus1", i))) for i in lines.ids]
+    edges = passive_branches(network)
     adjacency: dict = {}
     for e in edges:
         adjacency.setdefault(e[2], []).append(e)
@@ -262,12 +278,31 @@ def cycle_basis(network: Network) -> list:
     return cycles
 
 
+def tap_ratio(tab, entity: str) -> float:
+    """``Branches.tapRatio``: a missing, non-finite or non-positive tap is 1."""
+    if "tap_ratio" not in tab.static:
+        return 1.0
+    v = float(tab.value("tap_ratio", entity))
+    return v if math.isfinite(v) and v > 0.0 else 1.0
+
+
 def impedance(network: Network, component: str, entity: str, carrier: str) -> float:
-    """Reactance in an AC sub-network, resistance in a DC one, over v_nom^2 of bus0."""
+    """Per-unit impedance in a Kirchhoff row (``Cycles.impedance``,
+    Cycles.scala:154-193): reactance in an AC sub-network, resistance in a DC
+    one; a line's is referred to v_nom^2 of bus0, a transformer's to its own
+    rating and tap, z tap_ratio / s_nom.  The phase shift is not read: it
+    moves angles, not the optimised flows."""
     tab = network.table(component)
     raw = float(tab.value("r" if carrier == "DC" else "x", entity))
-    v = float(network.table("Bus").value("v_nom", str(tab.value("bus0", entity))))
-    return raw / (v * v)
+    if component == "Line":
+        v = float(network.table("Bus").value("v_nom", str(tab.value("bus0", entity))))
+        return raw / (v * v) if v > 0.0 else raw
+    if component == "Transformer":
+        s_nom = float(tab.value("s_nom", entity))
+        if not s_nom > 0.0:
+            raise UnsupportedNetwork(f"Transformer '{entity}' has s_nom = {s_nom}, which is its per-unit base")
+        return raw * tap_ratio(tab, entity) / s_nom
+    raise UnsupportedNetwork(f"{component} '{entity}' is a passive branch whose per-unit base is not known here")
 
 
 def build(network: Network) -> Model:
@@ -306,12 +341,14 @@ def build(network: Network) -> Model:
             pn = float(gens.value("p_nom", g))
             lo, hi = pn * gens.at("p_min_pu", g, t), pn * gens.at("p_max_pu", g, t)
             declare("Generator", g, t, min(lo, hi), max(lo, hi), gens.at("marginal_cost", g, t) * w)
-        for l in lines.ids:
-            if extendable(lines, l):
-                declare("Line", l, t, -math.inf, math.inf, 0.0)
-                continue
-            lim = float(lines.value("s_nom", l)) * lines.at("s_max_pu", l, t)
-            declare("Line", l, t, -lim, lim, 0.0)
+        for comp in PASSIVE:  # a symmetric rating on the flow p0 (Lopf.scala:174-186)
+            tab = network.table(comp)
+            for l in tab.ids:
+                if extendable(tab, l):
+                    declare(comp, l, t, -math.inf, math.inf, 0.0)
+                    continue
+                lim = float(tab.value("s_nom", l)) * tab.at("s_max_pu", l, t)
+                declare(comp, l, t, -lim, lim, 0.0)
         for k in links.ids:
             if extendable(links, k):
                 declare("Link", k, t, -math.inf, math.inf, links.at("marginal_cost", k, t) * w)
@@ -355,13 +392,14 @@ def build(network: Network) -> Model:
                     terms.append((columns[("StorageUnit-p_dispatch", u, t)], 1.0))
                     terms.append((columns[("StorageUnit-p_store", u, t)], -1.0))
             terms += [(columns[("Store-p", s_, t)], 1.0) for s_ in stores.ids if str(stores.value("bus", s_)) == bus]
-            for comp, tab in (("Line", lines), ("Link", links)):
+            for comp in PASSIVE + ("Link",):
+                tab = network.table(comp)
                 for e in tab.ids:
                     col = columns[(comp, e, t)]
                     if str(tab.value("bus0", e)) == bus:
                         terms.append((col, -1.0))
                     if str(tab.value("bus1", e)) == bus:
-                        terms.append((col, 1.0 if comp == "Line" else tab.at("efficiency", e, t)))
+                        terms.append((col, tab.at("efficiency", e, t) if comp == "Link" else 1.0))
             demand = sum(loads.at("p_set", d, t) for d in loads.ids if str(loads.value("bus", d)) == bus)
             b.equality_constraint(terms, demand)
             balance_rows[(bus, t)] = row
@@ -418,9 +456,9 @@ def build(network: Network) -> Model:
         for i in ids:
             cap = columns[(f"{c}-{nom}", i, -1)]
             for t in range(T):
-                if c == "Line":
+                if c in PASSIVE:
                     mx = tab.at("s_max_pu", i, t)
-                    pairs = [("Line", -mx, mx)]
+                    pairs = [(c, -mx, mx)]
                 elif c == "StorageUnit":
                     pairs = [("StorageUnit-p_dispatch", -math.inf, tab.at("p_max_pu", i, t)),
                              ("StorageUnit-p_store", -math.inf, -tab.at("p_min_pu", i, t)),
@@ -480,50 +518,53 @@ def solve(network: Network, params: PdhgParams = PdhgParams(), precision: int = 
 
 def sub_networks(network: Network) -> list:
     """Connected components of the buses over the passive branches, each
-    (carrier, [buses], [line ids]) -- ``Topology.subNetworks``."""
-    lines = network.table("Line")
+    (carrier, [buses], [(component, id) of its branches]) --
+    ``Topology.subNetworks``."""
+    branches = passive_branches(network)
     bus_tab = network.table("Bus")
     adjacency: dict = {b: [] for b in bus_tab.ids}
-    for l in lines.ids:
-        b0, b1 = str(lines.value("bus0", l)), str(lines.value("bus1", l))
-        adjacency[b0].append((l, b1))
-        adjacency[b1].append((l, b0))
+    for c, i, b0, b1 in branches:
+        adjacency[b0].append(((c, i), b1))
+        adjacency[b1].append(((c, i), b0))
     seen, out = set(), []
     for root in bus_tab.ids:
         if root in seen:
             continue
-        comp, stack, lids = [], [root], set()
+        comp, stack, keys = [], [root], set()
         seen.add(root)
         while stack:
             b = stack.pop()
             comp.append(b)
-            for l, nb in adjacency[b]:
-                lids.add(l)
+            for key, nb in adjacency[b]:
+                keys.add(key)
                 if nb not in seen:
                     seen.add(nb)
                     stack.append(nb)
-        out.append((str(bus_tab.value("carrier", root)), comp, [l for l in lines.ids if l in lids]))
+        out.append((str(bus_tab.value("carrier", root)), comp,
+                    [(c, i) for c, i, _, _ in branches if (c, i) in keys]))
     return out
 
 
-def lodf(network: Network, carrier: str, buses: list, lines: list, outages: Optional[set] = None):
-    """Line outage distribution factors of one sub-network (``Lodf.of``,
+def lodf(network: Network, carrier: str, buses: list, branches: list, outages: Optional[set] = None):
+    """Branch outage distribution factors of one sub-network (``Lodf.of``,
     modules/network-pf/.../Lodf.scala): PTDF = diag(b) A B^-1 with the first
     bus as reference (the factors do not depend on that choice), and
-    LODF[l, o] = PTDF_l(o) / (1 - PTDF_o(o)), -1 on the diagonal.  A bridge
-    (a denominator within 1e-7 of zero) has no post-outage flow: it is
-    refused if requested as a contingency and left unpopulated otherwise.
-    Returns (lines, factors m x m, populated per outage column)."""
-    m = len(lines)
+    LODF[l, o] = PTDF_l(o) / (1 - PTDF_o(o)), -1 on the diagonal, with b the
+    per-unit susceptance of the Kirchhoff rows.  A bridge (a denominator
+    within 1e-7 of zero) has no post-outage flow: it is refused if requested
+    as a contingency and left unpopulated otherwise.  ``branches`` are
+    (component, id) keys.  Returns (branches, factors m x m, populated per
+    outage column)."""
+    m = len(branches)
     if m == 0:
         return [], np.zeros((0, 0)), np.zeros(0, dtype=bool)
-    tab = network.table("Line")
     index = {b: i for i, b in enumerate(buses[1:])}
     n = len(index)
-    y = np.array([1.0 / impedance(network, "Line", l, carrier) for l in lines])
+    y = np.array([1.0 / impedance(network, c, i, carrier) for c, i in branches])
     A = np.zeros((m, n))
-    for k, l in enumerate(lines):
-        b0, b1 = str(tab.value("bus0", l)), str(tab.value("bus1", l))
+    for k, (c, i) in enumerate(branches):
+        tab = network.table(c)
+        b0, b1 = str(tab.value("bus0", i)), str(tab.value("bus1", i))
         if b0 in index:
             A[k, index[b0]] += 1.0
         if b1 in index:
@@ -533,44 +574,61 @@ def lodf(network: Network, carrier: str, buses: list, lines: list, outages: Opti
         np.linalg.cholesky(B)
     except np.linalg.LinAlgError as e:
         raise UnsupportedNetwork(f"sub-network {buses} has no unique power flow: {e}") from None
-    ptdf = (y[:, None] * A) @ np.linalg.inv(B)       # [m lines, n buses]
+    ptdf = (y[:, None] * A) @ np.linalg.inv(B)       # [m branches, n buses]
     branch_ptdf = ptdf @ A.T                           # [m, m]: flow on l per unit shifted across o
     factors = np.zeros((m, m))
     populated = np.zeros(m, dtype=bool)
-    for j, l in enumerate(lines):
+    for j, key in enumerate(branches):
         denominator = 1.0 - branch_ptdf[j, j]
-        requested = outages is None or l in outages
+        requested = outages is None or key in outages
         if abs(denominator) < 1e-7:
             if requested:
-                raise UnsupportedNetwork(f"Line '{l}' is a bridge: removing it disconnects the sub-network, "
-                                         "so it is not a credible contingency")
+                raise UnsupportedNetwork(f"{key[0]} '{key[1]}' is a bridge: removing it disconnects the "
+                                         "sub-network, so it is not a credible contingency")
             continue
         populated[j] = True
         factors[:, j] = branch_ptdf[:, j] / denominator
         factors[j, j] = -1.0
-    return lines, factors, populated
+    return branches, factors, populated
+
+
+def _outage_key(network: Network, o) -> tuple:
+    """An outage named by (component, id), or by id alone for a line (or a
+    transformer when no line has that name)."""
+    if isinstance(o, (tuple, list)):
+        key = (str(o[0]), str(o[1]))
+    else:
+        key = next(((c, str(o)) for c in PASSIVE if str(o) in network.table(c).ids), ("Line", str(o)))
+    if key[0] not in PASSIVE or key[1] not in network.table(key[0]).ids:
+        raise UnsupportedNetwork(f"'{key[1]}' is not a passive branch of this network, so it cannot be a contingency")
+    return key
 
 
 def build_sclopf(network: Network, outages: Optional[list] = None) -> Model:
     """``Sclopf.build`` (modules/network-lopf/.../Sclopf.scala:80-239): the
-    dispatch LP plus, per snapshot, monitored line l and contingency o != l
-    with a non-zero factor, the rating row
-    -s_nom_l s_max_pu <= f_l + LODF[l, o] f_o <= s_nom_l s_max_pu.
-    ``outages`` defaults to every line."""
+    dispatch LP plus, per snapshot, monitored passive branch l and
+    contingency o != l of its sub-network with a non-zero factor, the rating
+    row -s_nom_l s_max_pu <= f_l + LODF[l, o] f_o <= s_nom_l s_max_pu.
+    ``outages`` defaults to every passive branch."""
     base = build(network)
     if outages is not None and not outages:
         return base
-    lines_tab = network.table("Line")
-    subs = [(carrier, buses, lines, lodf(network, carrier, buses, lines, None if outages is None else set(outages)))
-            for carrier, buses, lines in sub_networks(network)]
-    requested = list(lines_tab.ids) if outages is None else list(outages)
-    for o in requested:
-        if o not in lines_tab.ids:
-            raise UnsupportedNetwork(f"'{o}' is not a passive branch of this network, so it cannot be a contingency")
+    for c in PASSIVE:  # before any factor is computed (Sclopf.scala:94-127)
+        tab = network.table(c)
+        ext = [i for i in tab.ids if extendable(tab, i)]
+        if ext:
+            raise UnsupportedNetwork(f"{c} '{ext[0]}' is extendable; the security rows cap post-contingency flow "
+                                     "at the rating in the file, so a secure dispatch would be priced against a "
+                                     "different network")
+    requested = [(c, i) for c, i, _, _ in passive_branches(network)] if outages is None else \
+        [_outage_key(network, o) for o in outages]
+    wanted = set(requested)
+    subs = [(carrier, buses, keys, lodf(network, carrier, buses, keys, wanted))
+            for carrier, buses, keys in sub_networks(network)]
     where = {}
-    for s_idx, (_, _, lines, (names, factors, populated)) in enumerate(subs):
-        for k, l in enumerate(names):
-            where[l] = (s_idx, k)
+    for s_idx, (_, _, _, (names, factors, populated)) in enumerate(subs):
+        for k, key in enumerate(names):
+            where[key] = (s_idx, k)
     p = base.problem
     b = LpBuilder(p.num_variables)
     for j in range(p.num_variables):
@@ -592,16 +650,17 @@ def build_sclopf(network: Network, outages: Optional[list] = None) -> Model:
         else:
             b.greater_than(terms, q)
     for t in range(len(network.snapshots)):
-        for s_idx, (_, _, lines, (names, factors, populated)) in enumerate(subs):
-            for k, l in enumerate(names):
-                limit = float(lines_tab.value("s_nom", l)) * lines_tab.at("s_max_pu", l, t)
-                col = base.columns[("Line", l, t)]
+        for s_idx, (_, _, _, (names, factors, populated)) in enumerate(subs):
+            for k, (c, l) in enumerate(names):
+                tab = network.table(c)
+                limit = float(tab.value("s_nom", l)) * tab.at("s_max_pu", l, t)
+                col = base.columns[(c, l, t)]
                 for o in requested:
-                    if o == l or where.get(o, (None,))[0] != s_idx:
+                    if o == (c, l) or where.get(o, (None,))[0] != s_idx:
                         continue
                     j = where[o][1]
                     factor = float(factors[k, j]) if populated[j] else 0.0
                     if factor != 0.0:
-                        b.constraint([(col, 1.0), (base.columns[("Line", o, t)], factor)], -limit, limit)
+                        b.constraint([(col, 1.0), (base.columns[(o[0], o[1], t)], factor)], -limit, limit)
     problem, translation = b.build()
     return Model(problem, translation, base.columns, base.balance_rows, base.cycles, base.objective_constant)

@@ -35,6 +35,9 @@ DEFAULTS = {
     "Load": {"p_set": 0.0},
     "Line": {"x": 0.0, "r": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "s_nom_extendable": False, "s_nom_min": 0.0,
              "s_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
+    "Transformer": {"x": 0.0, "r": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "tap_ratio": 1.0, "phase_shift": 0.0,
+                    "s_nom_extendable": False, "s_nom_min": 0.0, "s_nom_max": math.inf, "capital_cost": 0.0,
+                    "fom_cost": 0.0},
     "Link": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
              "p_nom_extendable": False, "p_nom_min": 0.0, "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
     "StorageUnit": {"p_nom": 0.0, "p_min_pu": -1.0, "p_max_pu": 1.0, "max_hours": 1.0, "efficiency_store": 1.0,

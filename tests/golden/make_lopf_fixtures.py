@@ -13,12 +13,12 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle", "ac-dc-meshed", "storage-hvdc",
-            "store-bank"]
+            "store-bank", "transformer-levels", "phase-shift"]
 # input tables only: component lists, their input series and the snapshots
 INPUTS = ["buses.csv", "carriers.csv", "generators.csv", "generators-p_max_pu.csv", "generators-p_min_pu.csv",
           "generators-marginal_cost.csv", "lines.csv", "links.csv", "loads.csv", "loads-p_set.csv", "snapshots.csv",
           "global_constraints.csv", "storage_units.csv", "storage_units-inflow.csv",
-          "storage_units-state_of_charge_set.csv", "stores.csv"]
+          "storage_units-state_of_charge_set.csv", "stores.csv", "transformers.csv"]
 
 
 def main(root):
@@ -34,7 +34,7 @@ def main(root):
         res = full["optimize"]
         keep = {k: res[k] for k in ("objective", "status", "condition", "generator_p", "line_p0", "link_p0",
                                     "storage_p_dispatch", "storage_p_store", "storage_state_of_charge",
-                                    "storage_spill", "store_e", "store_p", "objective_constant", "total_system_cost", "nominal_opt")
+                                    "storage_spill", "store_e", "store_p", "transformer_p0", "objective_constant", "total_system_cost", "nominal_opt")
                 if k in res}
         if "sclopf" in full:  # the security-constrained solve, with the outages PyPSA used
             keep["sclopf"] = {k: full["sclopf"][k] for k in ("branch_outages", "objective", "status", "generator_p",

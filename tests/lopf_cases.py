@@ -31,7 +31,7 @@ def frame_value(frame, t, column):
 
 
 NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle", "ac-dc-meshed",
-            "storage-hvdc", "store-bank"]
+            "storage-hvdc", "store-bank", "transformer-levels", "phase-shift"]
 
 
 def check_against_pypsa(solve, name="ac-dc-dispatch"):
@@ -47,7 +47,7 @@ def check_against_pypsa(solve, name="ac-dc-dispatch"):
     # dispatch and flows are compared where the optimum is unique (the
     # reference's LopfSuite does so on ac-dc-dispatch); elsewhere the objective
     # and the ratings are what is determined
-    unique = name in ("ac-dc-dispatch", "storage-cycle")
+    unique = name in ("ac-dc-dispatch", "storage-cycle", "transformer-levels", "phase-shift")
     for t in range(len(n.snapshots)):
         for g in gens.ids if unique else ():
             assert res.dispatch("Generator", g, t) == pytest.approx(frame_value(exp["generator_p"], t, g), abs=1e-3)
@@ -61,6 +61,12 @@ def check_against_pypsa(solve, name="ac-dc-dispatch"):
                               ("StorageUnit-state_of_charge", "storage_state_of_charge"),
                               ("StorageUnit-spill", "storage_spill")):
                 assert res.dispatch(comp, u, t) == pytest.approx(frame_value(exp[key], t, u), abs=1e-3), (comp, u, t)
+        for tr in n.table("Transformer").ids:  # a cycle spanning transformers (LopfSuite.scala:781-808)
+            flow = res.dispatch("Transformer", tr, t)
+            trs = n.table("Transformer")
+            assert abs(flow) <= res.capacity("Transformer", tr) * trs.at("s_max_pu", tr, t) + 1e-6
+            if unique:
+                assert flow == pytest.approx(frame_value(exp["transformer_p0"], t, tr), abs=1e-3)
         for st in n.table("Store").ids:  # energy and signed power (LopfSuite.scala:325-364)
             assert res.dispatch("Store-e", st, t) == pytest.approx(frame_value(exp["store_e"], t, st), abs=1e-4)
             assert res.dispatch("Store-p", st, t) == pytest.approx(frame_value(exp["store_p"], t, st), abs=1e-4)

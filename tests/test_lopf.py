@@ -35,8 +35,8 @@ def test_lodf_of_a_triangle():
     """Equal reactances: losing one side puts its whole flow on the other two,
     each seeing +-1 times it (a two-line path in series)."""
     n = X.network("sclopf-triangle")
-    [(carrier, buses, lines)] = lopf.sub_networks(n)
-    names, factors, populated = lopf.lodf(n, carrier, buses, lines)
+    [(carrier, buses, branches)] = lopf.sub_networks(n)
+    names, factors, populated = lopf.lodf(n, carrier, buses, branches)
     assert populated.all() and np.allclose(np.diag(factors), -1.0)
     assert np.allclose(np.abs(factors[~np.eye(3, dtype=bool)]), 1.0)
 
@@ -129,3 +129,86 @@ def test_store_features_not_built_are_refused(attr, value):
     st.static[attr] = {i: value for i in st.ids}
     with pytest.raises(lopf.UnsupportedNetwork):
         lopf.build(n)
+
+
+def test_a_transformer_is_referred_to_its_rating_and_tap():
+    n = X.network("transformer-levels")
+    tr = n.table("Transformer")
+    assert lopf.impedance(n, "Transformer", "t1", "AC") == pytest.approx(0.1 / 500.0)
+    tr.static["tap_ratio"] = {"t1": 1.05, "t2": -1.0}  # a non-positive tap reads as 1
+    assert lopf.impedance(n, "Transformer", "t1", "AC") == pytest.approx(0.1 * 1.05 / 500.0)
+    assert lopf.impedance(n, "Transformer", "t2", "AC") == pytest.approx(0.12 / 400.0)
+    tr.static["s_nom"]["t2"] = 0.0
+    with pytest.raises(lopf.UnsupportedNetwork, match="per-unit base"):
+        lopf.build(n)
+
+
+def test_the_phase_shift_leaves_the_optimised_flows_alone():
+    """PyPSA's optimised flows on phase-shift equal transformer-levels'
+    (LopfSuite.scala:1042-1090): the shift is not in the Kirchhoff rows."""
+    a, b = lopf.build(X.network("phase-shift")), lopf.build(X.network("transformer-levels"))
+    assert a.problem.constraint_matrix.nnz == b.problem.constraint_matrix.nnz
+    assert np.array_equal(a.problem.constraint_matrix.values, b.problem.constraint_matrix.values)
+    assert np.array_equal(a.problem.rhs, b.problem.rhs)
+
+
+def _flows(network, carrier, buses, branches, injection):
+    """DC power flow over the given branches: angles from B theta = P with the
+    first bus as reference, flow = b (theta0 - theta1)."""
+    index = {bus: i for i, bus in enumerate(buses[1:])}
+    y = np.array([1.0 / lopf.impedance(network, c, i, carrier) for c, i in branches])
+    A = np.zeros((len(branches), len(index)))
+    for k, (c, i) in enumerate(branches):
+        tab = network.table(c)
+        for port, sign in (("bus0", 1.0), ("bus1", -1.0)):
+            bus = str(tab.value(port, i))
+            if bus in index:
+                A[k, index[bus]] += sign
+    theta = np.linalg.solve(A.T @ (y[:, None] * A), np.array([injection[bus] for bus in buses[1:]]))
+    return y * (A @ theta)
+
+
+def test_outage_factors_match_a_power_flow_without_the_branch():
+    """f_l after losing o equals f_l + LODF[l, o] f_o before, over lines and
+    transformers together: the meshed transformer-levels network with a
+    second HV line added so that no branch is a bridge."""
+    from noaidi_b200.network.pypsa_csv import Table
+    n = X.network("transformer-levels")
+    lines = n.table("Line")
+    lines.ids.append("hv-b")
+    for attr, v in (("bus0", "hv1"), ("bus1", "hv2"), ("x", 0.7), ("s_nom", 600.0)):
+        lines.static.setdefault(attr, {})["hv-b"] = v
+    [(carrier, buses, branches)] = lopf.sub_networks(n)
+    assert ("Transformer", "t1") in branches and len(branches) == 5
+    names, factors, populated = lopf.lodf(n, carrier, buses, branches)
+    rng = np.random.default_rng(3)
+    injection = dict(zip(buses, rng.normal(size=len(buses))))
+    injection[buses[0]] -= sum(injection.values())
+    before = _flows(n, carrier, buses, branches, injection)
+    for j, o in enumerate(branches):
+        if not populated[j]:
+            continue
+        rest = [k for k in range(len(branches)) if k != j]
+        after = _flows(n, carrier, buses, [branches[k] for k in rest], injection)
+        expect = before[rest] + factors[rest, j] * before[j]
+        assert np.allclose(after, expect, atol=1e-9)
+    assert populated.sum() >= 2
+
+
+def test_sclopf_monitors_transformers_and_refuses_extendable_branches():
+    n = X.network("transformer-levels")
+    lines = n.table("Line")
+    lines.ids.append("hv-b")
+    for attr, v in (("bus0", "hv1"), ("bus1", "hv2"), ("x", 0.7), ("s_nom", 600.0)):
+        lines.static.setdefault(attr, {})["hv-b"] = v
+    plain = lopf.build(n)
+    secure = lopf.build_sclopf(n, [("Line", "hv"), ("Line", "hv-b")])
+    assert secure.problem.num_constraints > plain.problem.num_constraints
+    from oracle import oracle as O
+    a, b = O.solve(plain.problem, X.PARAMS), O.solve(secure.problem, X.PARAMS)
+    assert a.status.name == b.status.name == "OPTIMAL"
+    assert b.objective_value >= a.objective_value - 1e-6 * abs(a.objective_value)
+    with pytest.raises(lopf.UnsupportedNetwork, match="passive branch"):
+        lopf.build_sclopf(n, [("Link", "hv")])
+    with pytest.raises(lopf.UnsupportedNetwork, match="extendable"):
+        lopf.build_sclopf(X.network("ac-dc-meshed"))
