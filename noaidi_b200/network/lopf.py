@@ -36,6 +36,10 @@ with its conventions, since equivalence is judged against PyPSA's output:
   tie them to min_pu and max_pu times the capacity; the objective is the
   cost of the change, so the existing capacity's cost is subtracted.
 
+* standard types (noaidi_b200.network.standard_types): a typed line's or
+  transformer's impedance and a typed transformer's rating come from the
+  type library, expanded before anything is built.
+
 * transformers: passive branches like lines, rated by s_nom x s_max_pu and
   referred to their own base in Kirchhoff rows, z tap_ratio / s_nom
   (Cycles.scala:154-193); the phase shift moves angles, not the optimised
@@ -57,6 +61,7 @@ import numpy as np
 
 from ..prima.model import LpBuilder, LpProblem, Negated, RowTranslation
 from ..prima.types import LpSolution, PdhgParams, SolveStatus
+from . import standard_types
 from .pypsa_csv import Network
 
 HANDLED = {"Bus", "Carrier", "Generator", "Load", "Line", "Transformer", "Link", "GlobalConstraint", "SubNetwork",
@@ -82,6 +87,7 @@ class Model:
     balance_rows: dict  # (bus, t) -> row of the builder's constraints (before standard form)
     cycles: list
     objective_constant: float = 0.0  # cost of the capacity the network came with, extendables only
+    network: Optional[Network] = None  # what the LP was built from: standard types expanded
 
 
 @dataclass
@@ -113,7 +119,7 @@ class LopfResult:
         nom = NOMINAL[component]
         col = self.model.columns.get((f"{component}-{nom}", entity, -1))
         if col is None:
-            return float(self.network.table(component).value(nom, entity))
+            return float((self.model.network or self.network).table(component).value(nom, entity))
         return float(self.solution.primal[col])
 
 
@@ -306,6 +312,7 @@ def impedance(network: Network, component: str, entity: str, carrier: str) -> fl
 
 
 def build(network: Network) -> Model:
+    network = standard_types.expand(network)  # impedance named by type (Lopf.scala:73)
     _reject(network)
     T = len(network.snapshots)
     if T == 0:
@@ -383,24 +390,38 @@ def build(network: Network) -> Model:
     constant = sum(periodized_cost(tab, i) * float(tab.value(NOMINAL[c], i)) for c, tab, ids in expandable for i in ids)
     b.objective_offset(-constant)  # PyPSA reports the cost of the change (Lopf.scala:255-262)
 
+    # what each bus sees, grouped once rather than scanned per bus and snapshot
+    attached = {bus: {"gen": [], "unit": [], "store": [], "load": [], "branch": []} for bus in buses}
+    for g in gens.ids:
+        attached[str(gens.value("bus", g))]["gen"].append(g)
+    for u in units.ids:
+        attached[str(units.value("bus", u))]["unit"].append(u)
+    for s_ in stores.ids:
+        attached[str(stores.value("bus", s_))]["store"].append(s_)
+    for d in loads.ids:
+        attached[str(loads.value("bus", d))]["load"].append(d)
+    for comp in PASSIVE + ("Link",):
+        tab = network.table(comp)
+        for e in tab.ids:  # bus0 first, so a branch looping onto one bus lists -1 then its efficiency
+            attached[str(tab.value("bus0", e))]["branch"].append((comp, e, 0))
+            attached[str(tab.value("bus1", e))]["branch"].append((comp, e, 1))
+
     balance_rows, row = {}, 0
     for t in range(T):
         for bus in buses:
-            terms = [(columns[("Generator", g, t)], 1.0) for g in gens.ids if str(gens.value("bus", g)) == bus]
-            for u in units.ids:
-                if str(units.value("bus", u)) == bus:
-                    terms.append((columns[("StorageUnit-p_dispatch", u, t)], 1.0))
-                    terms.append((columns[("StorageUnit-p_store", u, t)], -1.0))
-            terms += [(columns[("Store-p", s_, t)], 1.0) for s_ in stores.ids if str(stores.value("bus", s_)) == bus]
-            for comp in PASSIVE + ("Link",):
-                tab = network.table(comp)
-                for e in tab.ids:
-                    col = columns[(comp, e, t)]
-                    if str(tab.value("bus0", e)) == bus:
-                        terms.append((col, -1.0))
-                    if str(tab.value("bus1", e)) == bus:
-                        terms.append((col, tab.at("efficiency", e, t) if comp == "Link" else 1.0))
-            demand = sum(loads.at("p_set", d, t) for d in loads.ids if str(loads.value("bus", d)) == bus)
+            at = attached[bus]
+            terms = [(columns[("Generator", g, t)], 1.0) for g in at["gen"]]
+            for u in at["unit"]:
+                terms.append((columns[("StorageUnit-p_dispatch", u, t)], 1.0))
+                terms.append((columns[("StorageUnit-p_store", u, t)], -1.0))
+            terms += [(columns[("Store-p", s_, t)], 1.0) for s_ in at["store"]]
+            for comp, e, port in at["branch"]:
+                col = columns[(comp, e, t)]
+                if port == 0:
+                    terms.append((col, -1.0))
+                else:
+                    terms.append((col, links.at("efficiency", e, t) if comp == "Link" else 1.0))
+            demand = sum(loads.at("p_set", d, t) for d in at["load"])
             b.equality_constraint(terms, demand)
             balance_rows[(bus, t)] = row
             row += 1
@@ -498,7 +519,7 @@ def build(network: Network) -> Model:
             b.less_than(terms, float(constraints.value("constant", gc)))
 
     problem, translation = b.build()
-    return Model(problem, translation, columns, balance_rows, cycles, constant)
+    return Model(problem, translation, columns, balance_rows, cycles, constant, network)
 
 
 def solve(network: Network, params: PdhgParams = PdhgParams(), precision: int = 64, device: int = 0,
@@ -610,6 +631,7 @@ def build_sclopf(network: Network, outages: Optional[list] = None) -> Model:
     contingency o != l of its sub-network with a non-zero factor, the rating
     row -s_nom_l s_max_pu <= f_l + LODF[l, o] f_o <= s_nom_l s_max_pu.
     ``outages`` defaults to every passive branch."""
+    network = standard_types.expand(network)  # factors come from the typed impedances (Sclopf.scala:84)
     base = build(network)
     if outages is not None and not outages:
         return base
@@ -663,4 +685,5 @@ def build_sclopf(network: Network, outages: Optional[list] = None) -> Model:
                     if factor != 0.0:
                         b.constraint([(col, 1.0), (base.columns[(o[0], o[1], t)], factor)], -limit, limit)
     problem, translation = b.build()
-    return Model(problem, translation, base.columns, base.balance_rows, base.cycles, base.objective_constant)
+    return Model(problem, translation, base.columns, base.balance_rows, base.cycles, base.objective_constant,
+                 network)

@@ -33,9 +33,11 @@ DEFAULTS = {
                   "p_nom_extendable": False, "committable": False, "carrier": "", "p_nom_min": 0.0,
                   "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
     "Load": {"p_set": 0.0},
-    "Line": {"x": 0.0, "r": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "s_nom_extendable": False, "s_nom_min": 0.0,
-             "s_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
-    "Transformer": {"x": 0.0, "r": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "tap_ratio": 1.0, "phase_shift": 0.0,
+    "Line": {"x": 0.0, "r": 0.0, "b": 0.0, "g": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "s_nom_extendable": False,
+             "s_nom_min": 0.0, "s_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0, "length": 0.0,
+             "num_parallel": 1.0},
+    "Transformer": {"x": 0.0, "r": 0.0, "b": 0.0, "g": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "tap_ratio": 1.0,
+                    "phase_shift": 0.0, "num_parallel": 1.0, "tap_position": 0.0, "tap_side": 0.0,
                     "s_nom_extendable": False, "s_nom_min": 0.0, "s_nom_max": math.inf, "capital_cost": 0.0,
                     "fom_cost": 0.0},
     "Link": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
@@ -65,6 +67,15 @@ class Table:
     def __len__(self) -> int:
         return len(self.ids)
 
+    def position(self, entity: str) -> int:
+        """The entity's column in the series arrays (an index kept in step
+        with ``ids``, which callers may append to)."""
+        index = self.__dict__.get("_index")
+        if index is None or len(index) != len(self.ids):
+            index = {i: k for k, i in enumerate(self.ids)}
+            self.__dict__["_index"] = index
+        return index[entity]
+
     def has(self, attribute: str) -> bool:
         return attribute in self.static or attribute in self.series
 
@@ -79,7 +90,7 @@ class Table:
     def at(self, attribute: str, entity: str, t: int) -> float:
         """A varying attribute at snapshot t: its series if there is one, else the static value."""
         if attribute in self.series:
-            return float(self.series[attribute][t, self.ids.index(entity)])
+            return float(self.series[attribute][t, self.position(entity)])
         return float(self.value(attribute, entity))
 
 
@@ -101,7 +112,8 @@ class Network:
 # Attributes that name other entities or labels: kept as text even when they
 # read as numbers (bus "0" is a name, not a zero).
 LABELS = frozenset({"bus", "bus0", "bus1", "bus2", "bus3", "carrier", "control", "type", "sub_network",
-                    "generator", "country", "location", "unit", "sense", "investment_period"})
+                    "generator", "country", "location", "unit", "sense", "investment_period", "mounting",
+                    "references", "model"})
 
 
 def _coerce(v, label: bool = False):
@@ -122,6 +134,17 @@ def _coerce(v, label: bool = False):
     return float(v)
 
 
+def read_table(path: str, component: str):
+    """One component list file (first column the names) as a Table of
+    static attributes, or None when it has no rows."""
+    df = pd.read_csv(path, dtype=str, keep_default_na=True)
+    if df.empty:
+        return None
+    ids = [str(v) for v in df[df.columns[0]]]
+    static = {col: {i: _coerce(v, col in LABELS) for i, v in zip(ids, df[col])} for col in df.columns[1:]}
+    return Table(component, ids, static)
+
+
 def read(folder: str, name: str = "") -> Network:
     snap = pd.read_csv(os.path.join(folder, "snapshots.csv"))
     label = "snapshot" if "snapshot" in snap.columns else snap.columns[0]
@@ -133,11 +156,10 @@ def read(folder: str, name: str = "") -> Network:
     for component, stem in LIST_NAMES.items():
         if f"{stem}.csv" not in files:
             continue
-        df = pd.read_csv(os.path.join(folder, f"{stem}.csv"), dtype=str, keep_default_na=True)
-        if df.empty:
+        static_table = read_table(os.path.join(folder, f"{stem}.csv"), component)
+        if static_table is None:
             continue
-        ids = [str(v) for v in df[df.columns[0]]]
-        static = {col: {i: _coerce(v, col in LABELS) for i, v in zip(ids, df[col])} for col in df.columns[1:]}
+        ids, static = static_table.ids, static_table.static
         series = {}
         for f in files:
             if f.startswith(stem + "-") and f.endswith(".csv"):

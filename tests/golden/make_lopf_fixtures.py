@@ -1,4 +1,5 @@
-"""Copies the input tables of PyPSA golden networks and the expected LOPF
+"""Copies PyPSA's standard type library into noaidi_b200/network/
+standard_types/, and the input tables of PyPSA golden networks and the expected LOPF
 results (objective, generator dispatch, line flows, storage trajectories,
 optimal capacities and the objective constant) from the reference's
 goldens (reference/goldens/{networks,results} in oluies/noaidi, generated by
@@ -13,24 +14,63 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle", "ac-dc-meshed", "storage-hvdc",
-            "store-bank", "transformer-levels", "phase-shift"]
+            "store-bank", "transformer-levels", "phase-shift", "standard-types", "scigrid-de"]
+# columns a network file may carry that no model reads (geometry, provenance)
+DROP = {"wkt_srid_4326", "osm_name", "operator", "ref", "from_relation", "wires", "cables", "length_m", "frequency",
+        "r_ohmkm", "x_ohmkm", "c_nfkm", "i_th_max_a", "voltage", "symbol", "under_construction", "tags", "osm_id",
+        "country", "geometry", "type_descr"}
+DROP_BUS = DROP | {"x", "y"}  # a bus's x and y are coordinates, a branch's x its reactance
 # input tables only: component lists, their input series and the snapshots
 INPUTS = ["buses.csv", "carriers.csv", "generators.csv", "generators-p_max_pu.csv", "generators-p_min_pu.csv",
           "generators-marginal_cost.csv", "lines.csv", "links.csv", "loads.csv", "loads-p_set.csv", "snapshots.csv",
           "global_constraints.csv", "storage_units.csv", "storage_units-inflow.csv",
-          "storage_units-state_of_charge_set.csv", "stores.csv", "transformers.csv"]
+          "storage_units-state_of_charge_set.csv", "stores.csv", "transformers.csv", "line_types.csv",
+          "transformer_types.csv"]
+
+
+# scigrid-de's results are not in the goldens; its PyPSA 1.2.4 (HiGHS) objective
+# is recorded in reference/generate_goldens.py:570-580, where two runs agree to
+# 2e-8 relative while the dispatch moves (a degenerate optimal face), so only
+# the objective gates.
+RECORDED = {
+    "scigrid-de": {"objective": 6684817.323607759, "status": "ok", "condition": "optimal",
+                   "dispatch_note": "degenerate optimum: PyPSA's own runs differ by up to 750 MW per generator "
+                                    "at the same cost; gate on the objective only"},
+}
+
+
+def _copy_table(src, dst):
+    """The table without its geometry and provenance columns, else verbatim."""
+    import pandas as pd
+    df = pd.read_csv(src, dtype=str, keep_default_na=False)
+    drop = DROP_BUS if os.path.basename(src) == "buses.csv" else DROP
+    if set(df.columns[1:]) & drop:
+        df.drop(columns=[c for c in df.columns[1:] if c in drop]).to_csv(dst, index=False)
+    else:
+        shutil.copyfile(src, dst)
 
 
 def main(root):
     goldens = os.path.join(root, "reference", "goldens")
+    # PyPSA's standard type library, which its CSV export omits: package data
+    library = os.path.join(os.path.dirname(HERE), "..", "noaidi_b200", "network", "standard_types")
+    os.makedirs(library, exist_ok=True)
+    for f in ("line_types.csv", "transformer_types.csv"):
+        shutil.copyfile(os.path.join(goldens, "standard_types", f), os.path.join(library, f))
     for name in NETWORKS:
         src = os.path.join(goldens, "networks", name)
         dst = os.path.join(HERE, "lopf", name)
         os.makedirs(dst, exist_ok=True)
         for f in INPUTS:
             if os.path.exists(os.path.join(src, f)):
-                shutil.copyfile(os.path.join(src, f), os.path.join(dst, f))
-        full = json.load(open(os.path.join(goldens, "results", f"{name}.json")))
+                _copy_table(os.path.join(src, f), os.path.join(dst, f))
+        results = os.path.join(goldens, "results", f"{name}.json")
+        if not os.path.exists(results):  # no results file: the optimum PyPSA's run recorded, if any
+            with open(os.path.join(dst, "expected.json"), "w") as f:
+                json.dump(RECORDED[name], f, indent=1)
+            print(name, "->", dst, "(recorded objective)")
+            continue
+        full = json.load(open(results))
         res = full["optimize"]
         keep = {k: res[k] for k in ("objective", "status", "condition", "generator_p", "line_p0", "link_p0",
                                     "storage_p_dispatch", "storage_p_store", "storage_state_of_charge",

@@ -31,7 +31,7 @@ def frame_value(frame, t, column):
 
 
 NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle", "ac-dc-meshed",
-            "storage-hvdc", "store-bank", "transformer-levels", "phase-shift"]
+            "storage-hvdc", "store-bank", "transformer-levels", "phase-shift", "standard-types"]
 
 
 def check_against_pypsa(solve, name="ac-dc-dispatch"):
@@ -47,7 +47,7 @@ def check_against_pypsa(solve, name="ac-dc-dispatch"):
     # dispatch and flows are compared where the optimum is unique (the
     # reference's LopfSuite does so on ac-dc-dispatch); elsewhere the objective
     # and the ratings are what is determined
-    unique = name in ("ac-dc-dispatch", "storage-cycle", "transformer-levels", "phase-shift")
+    unique = name in ("ac-dc-dispatch", "storage-cycle", "transformer-levels", "phase-shift", "standard-types")
     for t in range(len(n.snapshots)):
         for g in gens.ids if unique else ():
             assert res.dispatch("Generator", g, t) == pytest.approx(frame_value(exp["generator_p"], t, g), abs=1e-3)
@@ -130,4 +130,23 @@ def check_sclopf_triangle(solve):
     for t in range(len(n.snapshots)):
         for g in n.table("Generator").ids:
             assert res.dispatch("Generator", g, t) == pytest.approx(frame_value(exp["generator_p"], t, g), abs=1e-3)
+    return res
+
+
+SCIGRID = PdhgParams(eps_abs=1e-4, eps_rel=1e-4, max_iterations=100_000)
+
+
+def check_scigrid(solve, params=SCIGRID, tolerance=2e-4):
+    """LopfSuite.scala:519-555: scigrid-de -- 585 buses, 852 typed lines, 96
+    transformers, 38 storage units, 24 snapshots -- builds to 60,552
+    columns and 23,688 rows and solves to PyPSA's objective within the
+    tolerance; its dispatch is degenerate and is not compared."""
+    n = network("scigrid-de")
+    model = lopf.build(n)
+    assert model.problem.num_variables == 60_552 and model.problem.num_constraints == 23_688
+    sol = solve(model.problem, params)
+    res = lopf.LopfResult(n, model, sol)
+    assert res.status == SolveStatus.OPTIMAL
+    target = expected("scigrid-de")["objective"]
+    assert abs(res.objective - target) <= tolerance * abs(target), (res.objective, target)
     return res
