@@ -205,19 +205,49 @@ def run_batch(args, rank, world, dist, barrier):
             "nnz": int(sum(p.constraint_matrix.nnz for p in problems))}
 
 
+def profile_problem(workload: str, snapshots: int):
+    """The LP of a named workload: the DC-LOPF dispatch (optionally fewer
+    snapshots), the N-1 security-constrained LOPF, or the capacity-expansion
+    LOPF with storage over 8,760 hours."""
+    from noaidi_b200.prima import generators as G
+    if workload == "sclopf-n1":
+        return G.sclopf_n1(seed=0)
+    if workload == "expansion-storage":
+        from noaidi_b200.network.synthetic import expansion_storage
+        return expansion_storage(seed=0)
+    return G.dc_lopf(seed=0, **dict(WORKLOAD, snapshots=snapshots))
+
+
 def run_profile_case(args) -> None:
-    """A bounded run for profilers: the workload (optionally fewer snapshots)
+    """A bounded run for profilers and per-trial timing: the workload
     resident on the device, one plain PDHG solve capped at
-    --profile-iterations iterations in the chosen precision."""
-    from noaidi_b200.prima import PdhgParams, cuda, generators as G
-    problem = G.dc_lopf(seed=0, **dict(WORKLOAD, snapshots=args.profile_snapshots))
-    params = PdhgParams(eps_abs=EPS, eps_rel=EPS, max_iterations=args.profile_iterations)
-    resident = cuda.DeviceProblem(problem, params, precision=args.profile_precision)
-    s = resident.solve(params, want_solution=False)
-    print(json.dumps({"profile_case": True, "precision": args.profile_precision, "n": problem.num_variables,
-                      "m": problem.num_constraints, "nnz": problem.constraint_matrix.nnz,
-                      "iterations": s.iterations, "trials": s.trials,
-                      "us_per_trial": 1e3 * s.device_ms / max(1, s.trials)}), flush=True)
+    --profile-iterations iterations in the chosen precision, or with
+    --profile-mixed the FP32 refinement scheme to --profile-tolerance."""
+    from noaidi_b200.prima import MixedPrecisionParams, PdhgParams, cuda
+    t0 = time.perf_counter()
+    problem = profile_problem(args.profile_workload, args.profile_snapshots)
+    build_s = time.perf_counter() - t0
+    eps = args.profile_tolerance
+    params = PdhgParams(eps_abs=eps, eps_rel=eps, max_iterations=args.profile_iterations)
+    out = {"profile_case": True, "workload": args.profile_workload, "n": problem.num_variables,
+           "m": problem.num_constraints, "nnz": problem.constraint_matrix.nnz, "build_s": build_s, "eps": eps}
+    if args.profile_mixed:
+        ctx = cuda.Context(0, 32)
+        resident = cuda.DeviceProblem(problem, params, ctx=ctx)
+        r = resident.mixed_solve(params, MixedPrecisionParams(reduced_max_iterations=params.max_iterations),
+                                 scheme=cuda.MIXED_REFINEMENT, round_reduction=args.round_reduction,
+                                 want_solution=False)
+        s = r.solution
+        out.update(precision="fp32+fp64", reduced_iterations=r.reduced_iterations,
+                   refinement_iterations=r.refinement_iterations)
+    else:
+        resident = cuda.DeviceProblem(problem, params, precision=args.profile_precision)
+        s = resident.solve(params, want_solution=False)
+        out.update(precision=args.profile_precision)
+    out.update(status=s.status.name, objective=s.objective_value, iterations=s.iterations, trials=s.trials,
+               device_s=s.device_ms / 1e3, us_per_trial=1e3 * s.device_ms / max(1, s.trials))
+    resident.free()
+    print(json.dumps(out), flush=True)
 
 
 def main():
@@ -240,6 +270,9 @@ def main():
                     help="only run this many PDHG iterations of the workload (a bounded case for ncu) and exit")
     ap.add_argument("--profile-precision", type=int, default=32, choices=[32, 64])
     ap.add_argument("--profile-snapshots", type=int, default=WORKLOAD["snapshots"])
+    ap.add_argument("--profile-workload", default="dc-lopf", choices=["dc-lopf", "sclopf-n1", "expansion-storage"])
+    ap.add_argument("--profile-mixed", action="store_true")
+    ap.add_argument("--profile-tolerance", type=float, default=EPS)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
