@@ -1072,12 +1072,14 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
       // the step rule's two powers depend only on the iteration count: two
       // other warps evaluate them while the partials are being reduced
       __shared__ double s_pow[2];
+      const uint64_t t_in = (a.prof && threadIdx.x == 0) ? global_timer_ns() : 0;
       {
         const double t = (double)(c.iteration - c.period_base + 1);
         if (threadIdx.x == 32) s_pow[0] = pow(t, -0.3);
         if (threadIdx.x == 64) s_pow[1] = pow(t, -0.6);
       }
       reduce_partials<3>(a.partials, a.max_blocks, tm.nb, tm.s_part, red);
+      if (a.prof && threadIdx.x == 0) a.prof->reduce_b_ns += global_timer_ns() - t_in;
       if (threadIdx.x == 0) {
         c.trials += 1;
         c.total_trials += 1;
@@ -1269,7 +1271,7 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     __syncthreads();
     if (*((volatile int32_t *)&a.sync->abort)) return false;
     uint64_t t0 = 0;
-    if (threadIdx.x == 0) {
+    if (a.prof && threadIdx.x == 0) {
       t0 = global_timer_ns();
       if (a.prof->t_release) {
         a.prof->phase_ns[phase & 7] += t0 - a.prof->t_release;
@@ -1283,9 +1285,11 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      const uint64_t t1 = global_timer_ns();
-      a.prof->decide_ns += t1 - t0;
-      a.prof->t_release = t1;
+      if (a.prof) {
+        const uint64_t t1 = global_timer_ns();
+        a.prof->decide_ns += t1 - t0;
+        a.prof->t_release = t1;
+      }
       if (snap.phase == PH_DONE && a.queue) a.team_next[a.team] = atomicAdd(a.queue, 1);
     }
     __syncthreads();
@@ -1301,7 +1305,7 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
   __syncthreads();
   if (s_last) {
     __shared__ uint64_t s_t0;
-    if (threadIdx.x == 0) {
+    if (a.prof && threadIdx.x == 0) {
       s_t0 = global_timer_ns();
       const uint64_t tr = ldv(&a.prof->t_release);
       if (tr) {
@@ -1317,10 +1321,14 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     __syncthreads();
     if (phase != PH_A) publish_control(a, snap);
     if (threadIdx.x == 0 && snap.phase == PH_DONE && a.queue) a.team_next[a.team] = atomicAdd(a.queue, 1);
-    if (threadIdx.x == 0) {
+    if (a.prof && threadIdx.x == 0) {
       const uint64_t t1 = global_timer_ns();
       a.prof->decide_ns += t1 - s_t0;
       a.prof->t_release = t1;
+      if (phase == PH_B) {
+        a.prof->decide_b_ns += t1 - s_t0;
+        a.prof->decide_b_count += 1;
+      }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1634,6 +1642,13 @@ int32_t prepare_job(Ctx *c, Job<T> &j) {
   return ensure_tile_tables<T>(L, c->stream);
 }
 
+// Per-phase device timing, printed to stderr after each solve, when the
+// environment sets PRIMA_PHASE_TIMES.
+bool phase_times() {
+  static const bool on = std::getenv("PRIMA_PHASE_TIMES") != nullptr;
+  return on;
+}
+
 // Pdhg.Solve's initialise (Pdhg.scala:250-309) on the host -- the opening
 // step, primal weight and the projected start point -- and the Args, Control
 // and Sync records, with the iterate state at `base` laid out as S.
@@ -1724,7 +1739,7 @@ int32_t setup_job(Ctx *c, Job<T> &j, char *base, const StateLayout<T> &S, int bl
   a.max_blocks = blocks;
   a.ctl = (dev::Control *)(base + S.ctl);
   a.sync = (dev::Sync *)(base + S.sync);
-  a.prof = (dev::Prof *)(base + S.prof);
+  a.prof = phase_times() ? (dev::Prof *)(base + S.prof) : nullptr;
   a.tiles_k = (const int2 *)L.b_tiles[w][0].ptr;
   a.tiles_t = (const int2 *)L.b_tiles[w][1].ptr;
   a.ntiles_k = L.ntiles[w][0];
@@ -1766,7 +1781,7 @@ int32_t setup_job(Ctx *c, Job<T> &j, char *base, const StateLayout<T> &S, int bl
   std::memset(&sync, 0, sizeof(sync));
   PRIMA_CUDA_TRY(cudaMemcpyAsync(a.ctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
   PRIMA_CUDA_TRY(cudaMemcpyAsync(a.sync, &sync, sizeof(sync), cudaMemcpyHostToDevice, s));
-  PRIMA_CUDA_TRY(cudaMemsetAsync(a.prof, 0, sizeof(dev::Prof), s));
+  if (a.prof) PRIMA_CUDA_TRY(cudaMemsetAsync(a.prof, 0, sizeof(dev::Prof), s));
 
   dev::Params &P = a.P;
   P.eps_abs = p->eps_abs;
@@ -1823,13 +1838,18 @@ int32_t finish_job(Ctx *c, Job<T> &j, float kms, int blocks) {
   info->trials = ctl.total_trials;
   info->solve_ms = (int64_t)ms_since(j.t0);
   if (req.rounds) *req.rounds = ctl.rounds;
-  if (std::getenv("PRIMA_PHASE_TIMES")) {
+  if (a.prof) {
     dev::Prof prof;
     PRIMA_CUDA_TRY(cudaMemcpy(&prof, a.prof, sizeof(prof), cudaMemcpyDeviceToHost));
     static const char *names[8] = {"init", "A", "B", "F", "R", "W", "-", "R2"};
     std::fprintf(stderr, "[prima] blocks=%d tiles=%d/%d trials=%lld decide %.2f us/barrier:", blocks, a.ntiles_k,
                  a.ntiles_t, (long long)ctl.total_trials,
                  1e-3 * (double)prof.decide_ns / std::max<int64_t>(1, 2 * ctl.total_trials));
+    if (prof.decide_b_count) {
+      const double nb = (double)prof.decide_b_count;
+      std::fprintf(stderr, " | decide B %.2f us (partials %.2f) |", 1e-3 * (double)prof.decide_b_ns / nb,
+                   1e-3 * (double)prof.reduce_b_ns / nb);
+    }
     for (int k = 0; k < 8; k++)
       if (prof.phase_count[k])
         std::fprintf(stderr, " %s %.2f us x%lld", names[k], 1e-3 * (double)prof.phase_ns[k] / (double)prof.phase_count[k],

@@ -128,12 +128,17 @@ struct Sync {
 
 // Phase timing, kept by whichever block decides (one at a time): time from a
 // barrier's release to the last block's arrival at the next one, per phase
-// kind, and the deciding block's own time.
+// kind, and the deciding block's own time.  Only kept when asked for
+// (PRIMA_PHASE_TIMES): its read-modify-writes sit on the deciding thread's
+// path, and each one costs an L2 round trip while the team waits.
 struct Prof {
   uint64_t t_release;
   uint64_t decide_ns;
   uint64_t phase_ns[8];
   int64_t phase_count[8];
+  // the trial decision after phase B: all of it, and its partial reduction
+  uint64_t decide_b_ns, reduce_b_ns;
+  int64_t decide_b_count;
 };
 
 template <typename T>
