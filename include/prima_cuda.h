@@ -35,6 +35,7 @@ extern "C" {
 #define PRIMA_ERR_TIMEOUT 4 /* a bounded device-side wait gave up */
 #define PRIMA_ERR_CLOSED 5  /* handle unknown or its context closed */
 #define PRIMA_ERR_NO_DEVICE 6
+#define PRIMA_ERR_PARSE 7 /* a malformed input file (MpsParseException) */
 
 /* ---- SolveStatus (core/SolveResult.scala:9-18, same ordinals) ----------- */
 #define PRIMA_STATUS_OPTIMAL 0

@@ -27,7 +27,7 @@ from .types import (KktError, LpSolution, MixedPrecisionParams, MixedPrecisionRe
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "libprima_cuda.so")
 
-OK, ERR_INVALID_ARGUMENT, ERR_OUT_OF_MEMORY, ERR_CUDA, ERR_TIMEOUT, ERR_CLOSED, ERR_NO_DEVICE = range(7)
+OK, ERR_INVALID_ARGUMENT, ERR_OUT_OF_MEMORY, ERR_CUDA, ERR_TIMEOUT, ERR_CLOSED, ERR_NO_DEVICE, ERR_PARSE = range(8)
 MIXED_TWO_PASS, MIXED_REFINEMENT = 0, 1
 
 
@@ -84,8 +84,20 @@ class CMixedInfo(C.Structure):
                 ("refinement_rounds", C.c_int32), ("pad", C.c_int32)]
 
 
+class CMpsInfo(C.Structure):
+    _fields_ = [("num_variables", C.c_int32), ("num_constraints", C.c_int32), ("num_equalities", C.c_int32),
+                ("num_rows", C.c_int32), ("nnz", C.c_int64), ("num_integer_columns", C.c_int32), ("pad", C.c_int32)]
+
+
+class CPresolveInfo(C.Structure):
+    _fields_ = [("fixed_columns", C.c_int32), ("empty_columns", C.c_int32), ("empty_rows", C.c_int32),
+                ("singleton_rows", C.c_int32), ("proven_infeasible", C.c_int32),
+                ("unbounded_if_feasible", C.c_int32), ("passes", C.c_int32), ("reduced_variables", C.c_int32),
+                ("reduced_constraints", C.c_int32), ("reduced_equalities", C.c_int32), ("reduced_nnz", C.c_int64)]
+
+
 # Every exported symbol with its ctypes signature; the ABI test checks this
-# list against include/prima_cuda.h.
+# list against include/*.h.
 _H = C.c_int64
 _HP = C.POINTER(C.c_int64)
 _DP = C.POINTER(C.c_double)
@@ -128,6 +140,23 @@ SIGNATURES = {
                                         C.POINTER(CInfo)]),
     "prima_problem_mixed_solve": (C.c_int32, [_H, _H, C.POINTER(CParams), C.POINTER(CMixedParams), _IP, _DP, _DP,
                                               _DP, C.POINTER(CInfo), C.POINTER(CMixedInfo)]),
+    # the host model layer (include/prima_model.h)
+    "prima_mps_read": (C.c_int32, [C.c_char_p, C.c_int64, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "prima_mps_read_file": (C.c_int32, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "prima_mps_free": (None, [C.c_void_p]),
+    "prima_mps_get_info": (C.c_int32, [C.c_void_p, C.POINTER(CMpsInfo)]),
+    "prima_mps_get_problem": (C.c_int32, [C.c_void_p, C.POINTER(CLp)]),
+    "prima_mps_get_translation": (C.c_int32, [C.c_void_p, _IP, _IP, _IP]),
+    "prima_mps_name": (C.c_char_p, [C.c_void_p]),
+    "prima_mps_row_name": (C.c_char_p, [C.c_void_p, C.c_int32]),
+    "prima_mps_column_name": (C.c_char_p, [C.c_void_p, C.c_int32]),
+    "prima_mps_get_integer_columns": (C.c_int32, [C.c_void_p, _IP]),
+    "prima_presolve": (C.c_int32, [C.POINTER(CLp), C.c_int32, C.POINTER(C.c_void_p)]),
+    "prima_presolve_free": (None, [C.c_void_p]),
+    "prima_presolve_get_info": (C.c_int32, [C.c_void_p, C.POINTER(CPresolveInfo)]),
+    "prima_presolve_get_reduced": (C.c_int32, [C.c_void_p, C.POINTER(CLp)]),
+    "prima_presolve_get_maps": (C.c_int32, [C.c_void_p, _IP, _IP]),
+    "prima_presolve_restore": (C.c_int32, [C.c_void_p, _DP, _DP, _DP, _DP, _DP, _DP]),
 }
 
 _lib = None
@@ -172,6 +201,20 @@ def to_c_params(p: PdhgParams) -> CParams:
                    p.scaling.ruiz_iterations, int(p.scaling.apply_pock_chambolle), p.scaling.pock_chambolle_alpha,
                    p.infeasibility_tolerance, p.restart_sufficient_reduction, p.restart_necessary_reduction,
                    p.restart_artificial_fraction, p.primal_weight_smoothing)
+
+
+def lp_from_view(v: CLp) -> LpProblem:
+    """An LpProblem copied out of a prima_lp view the library owns."""
+    n, m = v.num_variables, v.num_constraints
+
+    def arr(ptr, k, dtype):
+        return np.ctypeslib.as_array(ptr, shape=(k,)).astype(dtype, copy=True) if k else np.zeros(0, dtype)
+
+    rp = arr(v.row_ptr, m + 1, np.int32)
+    nnz = int(rp[-1])
+    K = SparseMatrix(m, n, rp, arr(v.col_idx, nnz, np.int32), arr(v.values, nnz, np.float64))
+    return LpProblem(arr(v.objective, n, np.float64), K, arr(v.rhs, m, np.float64), v.num_equalities,
+                     arr(v.lower, n, np.float64), arr(v.upper, n, np.float64), v.objective_offset)
 
 
 class _LpView:

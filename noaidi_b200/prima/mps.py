@@ -1,11 +1,13 @@
-"""MPS reader for the linear-programming subset: ``MpsReader``
+"""The MPS reader: ``MpsReader``
 (modules/prima-mps/src/main/scala/org/noaidi/prima/mps/MpsReader.scala), the
-on-disk format in front of the device solve.
+on-disk format in front of the device solve, run by the C++ reader in
+libprima_cuda.so (``prima_mps_read``, include/prima_model.h).
 
 The conventions are the reference's, each of which changes the LP a file
 means if done differently:
 
-* whitespace-separated tokens, not fixed columns;
+* whitespace-separated tokens, not fixed columns; lines end at LF, CR or
+  CR LF; numbers follow ``java.lang.Double.parseDouble``'s grammar;
 * the first ``N`` row is the objective, later ``N`` rows are free and dropped;
 * an ``RHS`` entry on the objective row is the negated objective constant;
 * ``MI`` sets only the lower bound to -infinity;
@@ -20,11 +22,15 @@ means if done differently:
 """
 from __future__ import annotations
 
-import math
+import ctypes as C
+import os
 from dataclasses import dataclass
 from typing import Iterable, Optional
 
-from .model import LpBuilder, LpProblem, RowTranslation
+import numpy as np
+
+from . import cuda
+from .model import Direct, LpProblem, Negated, Range, RowTranslation
 
 
 class MpsParseError(ValueError):
@@ -52,200 +58,57 @@ class MpsInstance:
             return None
 
 
-class _Row:
-    __slots__ = ("name", "sense", "rhs", "range", "entries")
-
-    def __init__(self, name: str, sense: str):
-        self.name, self.sense, self.rhs, self.range, self.entries = name, sense, 0.0, None, []
+def _text(b: Optional[bytes]) -> str:
+    return "" if b is None else b.decode("utf-8", "surrogateescape")
 
 
-class _Col:
-    __slots__ = ("name", "index", "lower", "upper", "objective", "integer", "lower_explicit")
-
-    def __init__(self, name: str, index: int):
-        self.name, self.index = name, index
-        self.lower, self.upper, self.objective = 0.0, math.inf, 0.0
-        self.integer = self.lower_explicit = False
-
-
-def read_file(path: str) -> MpsInstance:
-    import os
-    with open(path) as f:
-        return read_lines(f, os.path.basename(path))
+def _instance(lib, code: int, handle: C.c_void_p) -> MpsInstance:
+    if code != cuda.OK:
+        msg = lib.prima_last_error().decode("utf-8", "surrogateescape")
+        if code == cuda.ERR_PARSE:
+            raise MpsParseError(msg)
+        if code == cuda.ERR_INVALID_ARGUMENT:
+            raise ValueError(msg)
+        raise cuda.PrimaError(code, msg)
+    h = handle.value
+    try:
+        info = cuda.CMpsInfo()
+        cuda._check(lib.prima_mps_get_info(h, C.byref(info)))
+        view = cuda.CLp()
+        cuda._check(lib.prima_mps_get_problem(h, C.byref(view)))
+        problem = cuda.lp_from_view(view)
+        k = info.num_rows
+        kind, first, second = (np.zeros(k, np.int32) for _ in range(3))
+        cuda._check(lib.prima_mps_get_translation(h, cuda._ip(kind), cuda._ip(first), cuda._ip(second)))
+        rows = [Direct(int(a)) if t == 0 else Negated(int(a)) if t == 1 else Range(int(a), int(b))
+                for t, a, b in zip(kind, first, second)]
+        integers = np.zeros(info.num_integer_columns, np.int32)
+        cuda._check(lib.prima_mps_get_integer_columns(h, cuda._ip(integers)))
+        return MpsInstance(_text(lib.prima_mps_name(h)), problem, RowTranslation(rows),
+                           [_text(lib.prima_mps_row_name(h, i)) for i in range(k)],
+                           [_text(lib.prima_mps_column_name(h, j)) for j in range(info.num_variables)],
+                           frozenset(int(j) for j in integers))
+    finally:
+        lib.prima_mps_free(h)
 
 
 def read_string(content: str, fallback_name: str = "inline") -> MpsInstance:
-    return read_lines(content.splitlines(), fallback_name)
+    """``MpsReader.fromString``."""
+    lib = cuda.library()
+    data = content.encode("utf-8", "surrogateescape")
+    h = C.c_void_p()
+    code = lib.prima_mps_read(data, len(data), fallback_name.encode("utf-8", "surrogateescape"), C.byref(h))
+    return _instance(lib, code, h)
 
 
-def _number(token: str, line: str) -> float:
-    try:
-        return float(token)
-    except ValueError:
-        raise MpsParseError(f"'{token}' is not a number, in: '{line}'") from None
-
-
-def _pairs(fields, line: str, section: str):
-    if len(fields) % 2:
-        raise MpsParseError(f"{section} entry has an unpaired field: '{line}'")
-    return [(fields[i], _number(fields[i + 1], line)) for i in range(0, len(fields), 2)]
-
-
-def _check_objsense(token: str) -> None:
-    if token.upper().startswith("MAX"):
-        raise MpsParseError("OBJSENSE MAX is not supported; the solver minimises")
+def read_file(path: str) -> MpsInstance:
+    """``MpsReader.read(path)``: the file's base name is the fallback name."""
+    lib = cuda.library()
+    h = C.c_void_p()
+    code = lib.prima_mps_read_file(os.fsencode(path), C.byref(h))
+    return _instance(lib, code, h)
 
 
 def read_lines(lines: Iterable[str], fallback_name: str) -> MpsInstance:
-    """``MpsReader.fromLines`` (:91-235)."""
-    name, objective, obj_constant, section, integer_block = fallback_name, "", 0.0, "", False
-    rows: dict[str, _Row] = {}
-    cols: dict[str, _Col] = {}
-    free: set = set()
-
-    def column(cname: str) -> _Col:
-        if cname not in cols:
-            cols[cname] = _Col(cname, len(cols))
-        return cols[cname]
-
-    def row(rname: str, context: str) -> Optional[_Row]:
-        if rname in free or rname == objective:
-            return None
-        if rname not in rows:
-            raise MpsParseError(f"{context} refers to unknown row '{rname}'")
-        return rows[rname]
-
-    for raw in lines:
-        line = raw.rstrip("\n").replace("\t", " ")
-        if not line.strip() or line.startswith("*"):
-            continue
-        tokens = line.split()
-        if not line.startswith(" "):
-            section = tokens[0].upper()
-            if section == "NAME" and len(tokens) > 1:
-                name = tokens[1]
-            elif section == "OBJSENSE" and len(tokens) > 1:
-                _check_objsense(tokens[1])
-            continue
-        if section == "ROWS":
-            if len(tokens) < 2:
-                raise MpsParseError(f"malformed ROWS entry: '{line}'")
-            kind, rname = tokens[0].upper(), tokens[1]
-            if kind == "N":
-                if not objective:
-                    objective = rname
-                else:
-                    free.add(rname)
-            elif kind in ("L", "G", "E"):
-                rows[rname] = _Row(rname, kind)
-            else:
-                raise MpsParseError(f"unknown row type '{kind}' for row '{rname}'")
-        elif section == "COLUMNS":
-            if "'MARKER'" in tokens:
-                if any(t.upper() == "'INTORG'" for t in tokens):
-                    integer_block = True
-                elif any(t.upper() == "'INTEND'" for t in tokens):
-                    integer_block = False
-                continue
-            if len(tokens) < 3:
-                raise MpsParseError(f"malformed COLUMNS entry: '{line}'")
-            col = column(tokens[0])
-            if integer_block:
-                col.integer = True
-            for rname, value in _pairs(tokens[1:], line, "COLUMNS"):
-                if rname == objective:
-                    col.objective += value
-                elif rname not in free:
-                    r = row(rname, "COLUMNS")
-                    if r is not None:
-                        r.entries.append((col.index, value))
-        elif section in ("RHS", "RANGES"):
-            fields = tokens[1:] if len(tokens) % 2 == 1 else tokens
-            for rname, value in _pairs(fields, line, section):
-                if section == "RHS":
-                    if rname == objective:
-                        obj_constant = -value
-                    elif rname not in free:
-                        r = row(rname, "RHS")
-                        if r is not None:
-                            r.rhs = value
-                else:
-                    r = row(rname, "RANGES")
-                    if r is not None:
-                        r.range = value
-        elif section == "BOUNDS":
-            if len(tokens) < 2:
-                raise MpsParseError(f"malformed BOUNDS entry: '{line}'")
-            kind = tokens[0].upper()
-            valueless = kind in ("FR", "MI", "PL", "BV")
-            candidates = tokens[1:] if valueless else tokens[1:max(2, len(tokens) - 1)]
-            cname = next((t for t in candidates if t in cols), None)
-            if cname is None:
-                raise MpsParseError(f"BOUNDS names no column declared in COLUMNS (tried {', '.join(candidates)}) "
-                                    f"in: '{line}'")
-            if len(tokens) > 4:
-                raise MpsParseError(f"BOUNDS entry carries more fields than one bound uses: '{line}'")
-            col = cols[cname]
-            if kind == "UP":
-                value = _number(tokens[-1], line)
-                col.upper = value
-                if value < 0.0 and not col.lower_explicit:
-                    col.lower = -math.inf
-            elif kind == "LO":
-                col.lower, col.lower_explicit = _number(tokens[-1], line), True
-            elif kind == "FX":
-                value = _number(tokens[-1], line)
-                col.lower = col.upper = value
-                col.lower_explicit = True
-            elif kind == "FR":
-                col.lower, col.upper, col.lower_explicit = -math.inf, math.inf, True
-            elif kind == "MI":
-                col.lower, col.lower_explicit = -math.inf, True
-            elif kind == "PL":
-                col.upper = math.inf
-            elif kind == "BV":
-                col.lower, col.upper, col.integer, col.lower_explicit = 0.0, 1.0, True, True
-            elif kind == "LI":
-                col.lower, col.integer, col.lower_explicit = _number(tokens[-1], line), True, True
-            elif kind == "UI":
-                col.upper, col.integer = _number(tokens[-1], line), True
-            else:
-                raise MpsParseError(f"unknown bound type '{kind}' on '{cname}'")
-        elif section == "OBJSENSE":
-            _check_objsense(tokens[0])
-        elif section in ("ENDATA", ""):
-            pass
-        else:
-            raise MpsParseError(f"unexpected data in section '{section}'")
-
-    if not objective:
-        raise MpsParseError("no objective row (an N row) was declared")
-    return _build(name, obj_constant, list(rows.values()), list(cols.values()))
-
-
-def _bracket(r: _Row) -> tuple[float, float]:
-    """Row sense, right-hand side and optional range as two-sided bounds (:300-316)."""
-    if r.range is None:
-        return {"L": (-math.inf, r.rhs), "G": (r.rhs, math.inf), "E": (r.rhs, r.rhs)}[r.sense]
-    width = abs(r.range)
-    if r.sense == "G":
-        return r.rhs, r.rhs + width
-    if r.sense == "L":
-        return r.rhs - width, r.rhs
-    return (r.rhs, r.rhs + width) if r.range >= 0.0 else (r.rhs - width, r.rhs)
-
-
-def _build(name: str, constant: float, rows: list, cols: list) -> MpsInstance:
-    b = LpBuilder(len(cols))
-    b.objective_offset(constant)
-    for c in cols:
-        b.objective_coefficient(c.index, c.objective)
-        if c.lower > c.upper:
-            raise MpsParseError(f"column '{c.name}' has empty bounds [{c.lower}, {c.upper}]")
-        b.bounds(c.index, c.lower, c.upper)
-    for r in rows:
-        lo, hi = _bracket(r)
-        b.constraint(r.entries, lo, hi)
-    problem, translation = b.build()
-    return MpsInstance(name, problem, translation, [r.name for r in rows], [c.name for c in cols],
-                       frozenset(c.index for c in cols if c.integer))
+    """``MpsReader.fromLines``."""
+    return read_string("\n".join(line.rstrip("\r\n") for line in lines), fallback_name)
