@@ -145,7 +145,8 @@ def _reject(network: Network) -> None:
     gens = network.table("Generator")
     for g in gens.ids:
         if bool(gens.value("committable", g)) is True:
-            raise UnsupportedNetwork(f"Generator '{g}' is committable; unit commitment is not a dispatch LP")
+            raise UnsupportedNetwork(f"Generator '{g}' is committable; unit commitment is not a dispatch LP "
+                                     "(noaidi_b200.network.unit_commitment solves it as a MILP)")
     if "p_set" in gens.series and np.isfinite(gens.series["p_set"]).any():
         raise UnsupportedNetwork("a generator has a p_set, which fixes its dispatch; the dispatch model does not")
     su = network.table("StorageUnit")

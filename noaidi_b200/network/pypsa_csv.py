@@ -31,7 +31,11 @@ DEFAULTS = {
     "Bus": {"v_nom": 1.0, "carrier": "AC"},
     "Generator": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
                   "p_nom_extendable": False, "committable": False, "carrier": "", "p_nom_min": 0.0,
-                  "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
+                  "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0, "start_up_cost": 0.0,
+                  "shut_down_cost": 0.0, "min_up_time": 0.0, "min_down_time": 0.0, "up_time_before": 1.0,
+                  "down_time_before": 0.0, "stand_by_cost": 0.0, "marginal_cost_quadratic": 0.0,
+                  "ramp_limit_up": math.nan, "ramp_limit_down": math.nan, "ramp_limit_start_up": math.nan,
+                  "ramp_limit_shut_down": math.nan},
     "Load": {"p_set": 0.0},
     "Line": {"x": 0.0, "r": 0.0, "b": 0.0, "g": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "s_nom_extendable": False,
              "s_nom_min": 0.0, "s_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0, "length": 0.0,

@@ -14,7 +14,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 NETWORKS = ["ac-dc-dispatch", "ac-dc-co2", "lodf-mesh", "sclopf-triangle", "storage-cycle", "ac-dc-meshed", "storage-hvdc",
-            "store-bank", "transformer-levels", "phase-shift", "standard-types", "scigrid-de"]
+            "store-bank", "transformer-levels", "phase-shift", "standard-types", "scigrid-de", "unit-commitment"]
 # columns a network file may carry that no model reads (geometry, provenance)
 DROP = {"wkt_srid_4326", "osm_name", "operator", "ref", "from_relation", "wires", "cables", "length_m", "frequency",
         "r_ohmkm", "x_ohmkm", "c_nfkm", "i_th_max_a", "voltage", "symbol", "under_construction", "tags", "osm_id",
@@ -74,7 +74,7 @@ def main(root):
         res = full["optimize"]
         keep = {k: res[k] for k in ("objective", "status", "condition", "generator_p", "line_p0", "link_p0",
                                     "storage_p_dispatch", "storage_p_store", "storage_state_of_charge",
-                                    "storage_spill", "store_e", "store_p", "transformer_p0", "objective_constant", "total_system_cost", "nominal_opt")
+                                    "storage_spill", "store_e", "store_p", "transformer_p0", "generator_status", "objective_constant", "total_system_cost", "nominal_opt")
                 if k in res}
         if "sclopf" in full:  # the security-constrained solve, with the outages PyPSA used
             keep["sclopf"] = {k: full["sclopf"][k] for k in ("branch_outages", "objective", "status", "generator_p",
