@@ -1241,6 +1241,16 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
 
 constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~seconds; a phase takes microseconds
 
+// The team barrier's generation as this block last saw it.  Read from the
+// Sync record once when a solve starts -- no barrier of that solve can have
+// released before every block of the team arrived at it -- and counted up at
+// each barrier after, so that arriving costs one atomic rather than a load of
+// the generation followed by the atomic.
+__device__ __forceinline__ unsigned &barrier_generation() {
+  __shared__ unsigned s_gen;
+  return s_gen;
+}
+
 template <typename T>
 __device__ __forceinline__ void publish_control(const Args<T> &a, const Control &snap) {
   const unsigned *src = (const unsigned *)&snap;
@@ -1264,7 +1274,6 @@ __device__ __forceinline__ void load_control(const Args<T> &a, Control &snap) {
 // with __syncthreads and keeps its Control in shared memory.
 template <typename T>
 __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const Team &tm) {
-  __shared__ unsigned s_gen;
   __shared__ int s_last, s_ok;
   __shared__ double s_red[kMaxQ];
   if (tm.nb == 1) {
@@ -1295,9 +1304,9 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     __syncthreads();
     return true;
   }
+  unsigned &s_gen = barrier_generation();
   __syncthreads();
   if (threadIdx.x == 0) {
-    s_gen = ld_acquire(&a.sync->gen);
     const unsigned old = atom_add_acq_rel(&a.sync->count, 1u);
     s_last = old == (unsigned)(tm.nb - 1);
     s_ok = 1;
@@ -1336,6 +1345,7 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
       a.sync->count = 0;
       __threadfence();
       st_release(&a.sync->gen, s_gen + 1);
+      s_gen += 1;
     }
   } else if (threadIdx.x == 0) {
     unsigned long long spins = 0;
@@ -1351,6 +1361,7 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
       }
       __nanosleep(32);
     }
+    s_gen += 1;
     if (phase == PH_A) snap.phase = PH_B;
   }
   __syncthreads();
@@ -1364,6 +1375,7 @@ template <typename T>
 __device__ __forceinline__ bool run_solve(const Args<T> &a, const Team &tm, Control &snap, HotShared &hs,
                                           unsigned &par, unsigned char *s_dyn) {
   T *s_prod = reinterpret_cast<T *>(s_dyn);
+  if (threadIdx.x == 0 && tm.nb > 1) barrier_generation() = ld_acquire(&a.sync->gen);
   load_control(a, snap);  // (syncs the block)
   bool alive = true;
   for (;;) {
