@@ -1307,6 +1307,10 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
   unsigned &s_gen = barrier_generation();
   __syncthreads();
   if (threadIdx.x == 0) {
+    if (a.prof) {
+      const uint64_t tr = ldv(&a.prof->t_release);
+      if (tr) atomicAdd((unsigned long long *)&a.prof->arrive_ns[phase & 7], (unsigned long long)(global_timer_ns() - tr));
+    }
     const unsigned old = atom_add_acq_rel(&a.sync->count, 1u);
     s_last = old == (unsigned)(tm.nb - 1);
     s_ok = 1;
@@ -1862,6 +1866,11 @@ int32_t finish_job(Ctx *c, Job<T> &j, float kms, int blocks) {
       std::fprintf(stderr, " | decide B %.2f us (partials %.2f) |", 1e-3 * (double)prof.decide_b_ns / nb,
                    1e-3 * (double)prof.reduce_b_ns / nb);
     }
+    std::fprintf(stderr, " | mean arrival:");
+    for (int k = 0; k < 8; k++)
+      if (prof.phase_count[k] && prof.arrive_ns[k])
+        std::fprintf(stderr, " %s %.2f us", names[k], 1e-3 * (double)prof.arrive_ns[k] / ((double)prof.phase_count[k] * blocks));
+    std::fprintf(stderr, " |");
     for (int k = 0; k < 8; k++)
       if (prof.phase_count[k])
         std::fprintf(stderr, " %s %.2f us x%lld", names[k], 1e-3 * (double)prof.phase_ns[k] / (double)prof.phase_count[k],

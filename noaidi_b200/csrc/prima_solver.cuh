@@ -139,6 +139,7 @@ struct Prof {
   // the trial decision after phase B: all of it, and its partial reduction
   uint64_t decide_b_ns, reduce_b_ns;
   int64_t decide_b_count;
+  uint64_t arrive_ns[8];  // every block's arrival after the release, summed
 };
 
 template <typename T>
