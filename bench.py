@@ -169,6 +169,55 @@ def run_reference(args) -> None:
 BATCH_EPS = 1e-6
 
 
+def _batch_specs(seed: int, count: int, min_buses=100, max_buses=2000, min_snapshots=24, max_snapshots=168):
+    """The (seed, buses, lines, generators, snapshots, load scale) of each
+    instance of ``generators.lopf_batch``, drawn the same way."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        B = int(rng.integers(min_buses, max_buses + 1))
+        T = int(rng.integers(min_snapshots, max_snapshots + 1))
+        scale = float(rng.uniform(0.6, 0.95))
+        out.append((seed + i, B, (3 * B) // 2, B // 2, T, scale))
+    return out
+
+
+def _oracle_seconds_per_iteration(spec, iters: int = 16) -> float:
+    """One instance on one host core: FP64 PDHG iterations of the oracle,
+    setup taken out by differencing against a one-iteration run."""
+    from noaidi_b200.prima import PdhgParams, generators as G
+    from oracle import oracle as O
+    problem = G.dc_lopf(*spec)
+    t = time.perf_counter()
+    O.solve(problem, PdhgParams(eps_abs=BATCH_EPS, eps_rel=BATCH_EPS, max_iterations=1))
+    t1 = time.perf_counter() - t
+    t = time.perf_counter()
+    s = O.solve(problem, PdhgParams(eps_abs=BATCH_EPS, eps_rel=BATCH_EPS, max_iterations=iters))
+    return max(time.perf_counter() - t - t1, 1e-9) / max(1, s.iterations - 1)
+
+
+def batch_cpu_baseline(specs, nnz, iterations, sample: int = 8):
+    """``PrimaZio.solveAll``'s CPU shape -- one single-threaded FP64 solve per
+    host core at a time -- estimated from a bounded sample: up to ``sample``
+    instances spread over the sizes are timed per iteration in parallel
+    processes (spawned, so none inherits a GPU context); seconds per
+    iteration per nonzero from them, times each instance's nonzeros and the
+    iterations its device solve took, summed over the instances and shared
+    over the cores."""
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    order = sorted(range(len(specs)), key=lambda i: nnz[i])
+    picks = sorted({order[round(k * (len(order) - 1) / max(1, sample - 1))] for k in range(min(sample, len(order)))})
+    with mp.get_context("spawn").Pool(min(cores, len(picks))) as pool:
+        per_iter = pool.map(_oracle_seconds_per_iteration, [specs[i] for i in picks])
+    rate = float(np.median([t / nnz[i] for t, i in zip(per_iter, picks)]))
+    cpu_seconds = sum(rate * nnz[i] * iterations[i] for i in range(len(specs))) / cores
+    return {"value": len(specs) / cpu_seconds, "unit": "LPs/s", "cores": cores, "kind": "port",
+            "sample": f"{len(picks)} of the instances timed over 16 FP64 PDHG iterations each on the oracle, one "
+                      f"process per instance; {rate * 1e9:.2f} ns per nonzero-iteration extrapolated to every "
+                      f"instance's nonzeros and the iterations its device solve took, over {cores} cores"}
+
+
 def run_batch(args, rank, world, dist, barrier):
     """Config 3: an uneven sweep of ``--batch`` DC-LOPF instances (buses
     U{100..2000}, snapshots U{24..168}, load scale U[0.6, 0.95], seeded), FP32
@@ -196,7 +245,12 @@ def run_batch(args, rank, world, dist, barrier):
     ctx.close()
     its = [r.reduced_iterations + r.refinement_iterations for r in res]
     statuses = sorted({r.solution.status.name for r in res})
+    cpu = None
+    if rank == 0 and res and not args.skip_cpu:
+        specs = _batch_specs(0, args.batch)
+        cpu = batch_cpu_baseline([specs[i] for i in mine], [problems[i].constraint_matrix.nnz for i in mine], its)
     return {"workload": f"config 3: {args.batch} uneven DC-LOPF instances, FP32 refinement to {BATCH_EPS:g}",
+            "cpu_baseline": cpu,
             "instances": args.batch, "lps_per_s": args.batch / float(agg[0]), "seconds": float(agg[0]),
             "wall_seconds": float(agg[1]), "statuses_rank0": statuses,
             "iterations_rank0": {"min": int(min(its)), "median": float(np.median(its)), "max": int(max(its))}
