@@ -8,8 +8,9 @@ with its conventions, since equivalence is judged against PyPSA's output:
   p0 in p_nom x [p_min_pu, p_max_pu]; costs are marginal_cost x the
   snapshot's objective weighting (:148-196);
 * bus balance per snapshot and bus: generators inject, a branch takes p0 out
-  at bus0 and delivers efficiency x p0 at bus1 (1 for a line), loads on the
-  right-hand side (:281-333);
+  at bus0 and delivers efficiency x p0 at bus1 (1 for a line), and a
+  multi-port link efficiencyN x p0 at each further busN it names
+  (Topology.scala:175-227), loads on the right-hand side (:281-333);
 * Kirchhoff's voltage law over a cycle basis of the passive branches, one
   row per cycle per snapshot: sum(orientation x impedance x p0) = 0, with
   reactance in AC sub-networks and resistance in DC ones, referred to
@@ -53,6 +54,7 @@ dropped: a dropped component leaves a feasible LP for a different network.
 from __future__ import annotations
 
 import math
+import re
 from collections import deque
 from dataclasses import dataclass
 from typing import Optional
@@ -174,14 +176,43 @@ def _reject(network: Network) -> None:
         raise UnsupportedNetwork("a Store has a non-zero marginal_cost_quadratic; the objective here is linear")
     _reject_standing_loss(network, st)
     buses = set(network.table("Bus").ids)
+    links = network.table("Link")
+    if len(links):
+        for required in ("bus0", "bus1"):  # Topology.portsOf: a branch needs both endpoints
+            if required not in links.static:
+                raise UnsupportedNetwork(f"links has no '{required}' column; a branch needs both endpoints")
     for comp, ports in (("Generator", ("bus",)), ("Load", ("bus",)), ("StorageUnit", ("bus",)), ("Store", ("bus",)),
                         ("Line", ("bus0", "bus1")), ("Transformer", ("bus0", "bus1")),
-                        ("Link", ("bus0", "bus1"))):
+                        ("Link", tuple(link_ports(links)))):
         tab = network.table(comp)
         for i in tab.ids:
             for port in ports:
+                if port not in ("bus", "bus0", "bus1") and not _named(tab.value(port, i)):
+                    continue  # a later port a link leaves empty: not connected
                 if str(tab.value(port, i)) not in buses:
                     raise UnsupportedNetwork(f"{comp} '{i}' references unknown bus '{tab.value(port, i)}' via {port}")
+
+
+def _named(v) -> bool:
+    return isinstance(v, str) and v.strip() != ""
+
+
+def link_ports(links) -> list:
+    """``Topology.portsOf``: bus0, bus1 and any further busN columns of the
+    links, in port order (a multi-port link, PyPSA's ``bus2``...)."""
+    ports = [c for c in links.static if re.fullmatch(r"bus[0-9]+", c)]
+    return sorted(set(ports) | {"bus0", "bus1"}, key=lambda c: int(c[3:]))
+
+
+def port_efficiency(links, entity: str, port: str, t: int) -> float:
+    """``Topology.portEfficiency``: ``efficiency`` for bus1, ``efficiencyN``
+    for busN, a series over the static value; a missing or non-finite value
+    is lossless."""
+    attr = "efficiency" if port == "bus1" else f"efficiency{port[3:]}"
+    if attr not in links.series and attr not in links.static and attr != "efficiency":
+        return 1.0
+    v = links.at(attr, entity, t)
+    return v if math.isfinite(v) else 1.0
 
 
 NOMINAL = {"Generator": "p_nom", "Line": "s_nom", "Transformer": "s_nom", "Link": "p_nom", "StorageUnit": "p_nom",
@@ -403,9 +434,12 @@ def build(network: Network) -> Model:
         attached[str(loads.value("bus", d))]["load"].append(d)
     for comp in PASSIVE + ("Link",):
         tab = network.table(comp)
+        ports = link_ports(tab) if comp == "Link" else ["bus0", "bus1"]
         for e in tab.ids:  # bus0 first, so a branch looping onto one bus lists -1 then its efficiency
-            attached[str(tab.value("bus0", e))]["branch"].append((comp, e, 0))
-            attached[str(tab.value("bus1", e))]["branch"].append((comp, e, 1))
+            for port in ports:
+                bus = tab.value(port, e)
+                if _named(bus) and str(bus) in attached:
+                    attached[str(bus)]["branch"].append((comp, e, port))
 
     balance_rows, row = {}, 0
     for t in range(T):
@@ -418,10 +452,10 @@ def build(network: Network) -> Model:
             terms += [(columns[("Store-p", s_, t)], 1.0) for s_ in at["store"]]
             for comp, e, port in at["branch"]:
                 col = columns[(comp, e, t)]
-                if port == 0:
+                if port == "bus0":  # flow enters the branch at bus0
                     terms.append((col, -1.0))
-                else:
-                    terms.append((col, links.at("efficiency", e, t) if comp == "Link" else 1.0))
+                else:  # and arrives at every other port scaled by that port's efficiency
+                    terms.append((col, port_efficiency(links, e, port, t) if comp == "Link" else 1.0))
             demand = sum(loads.at("p_set", d, t) for d in at["load"])
             b.equality_constraint(terms, demand)
             balance_rows[(bus, t)] = row

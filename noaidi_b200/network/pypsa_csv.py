@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import math
 import os
+import re
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -145,7 +146,8 @@ def read_table(path: str, component: str):
     if df.empty:
         return None
     ids = [str(v) for v in df[df.columns[0]]]
-    static = {col: {i: _coerce(v, col in LABELS) for i, v in zip(ids, df[col])} for col in df.columns[1:]}
+    static = {col: {i: _coerce(v, col in LABELS or re.fullmatch(r"bus[0-9]+", col) is not None)
+                    for i, v in zip(ids, df[col])} for col in df.columns[1:]}
     return Table(component, ids, static)
 
 

@@ -235,3 +235,48 @@ def test_sclopf_expands_types_before_computing_outage_factors():
     assert model.problem.num_constraints > plain.problem.num_constraints
     a, b = O.solve(plain.problem, X.PARAMS), O.solve(model.problem, X.PARAMS)
     assert b.status.name == "OPTIMAL" and b.objective_value >= a.objective_value - 1e-6
+
+
+def _chp_network(efficiency2):
+    """Gas into a combined heat and power link: electricity out at 0.4, heat
+    at efficiency2; a heat dump takes what the heat load does not."""
+    from noaidi_b200.network.pypsa_csv import Network, Table
+    T = len(efficiency2)
+    series = {} if T == 1 else {"efficiency2": np.array([[e, np.nan] for e in efficiency2])}
+    tables = {
+        "Bus": Table("Bus", ["gas", "elec", "heat"], {}),
+        "Generator": Table("Generator", ["supply", "dump"], {
+            "bus": {"supply": "gas", "dump": "heat"}, "p_nom": {"supply": 1000.0, "dump": 1000.0},
+            "p_min_pu": {"supply": 0.0, "dump": -1.0}, "p_max_pu": {"supply": 1.0, "dump": 0.0},
+            "marginal_cost": {"supply": 20.0, "dump": 0.0}}),
+        "Link": Table("Link", ["chp", "boiler"], {
+            "bus0": {"chp": "gas", "boiler": "gas"}, "bus1": {"chp": "elec", "boiler": "elec"},
+            "bus2": {"chp": "heat", "boiler": ""}, "p_nom": {"chp": 1000.0, "boiler": 1000.0},
+            "efficiency": {"chp": 0.4, "boiler": 0.3}, "efficiency2": {"chp": efficiency2[0], "boiler": np.nan},
+            "marginal_cost": {"chp": 0.0, "boiler": 50.0}}, series),
+        "Load": Table("Load", ["e", "h"], {"bus": {"e": "elec", "h": "heat"}, "p_set": {"e": 40.0, "h": 30.0}}),
+    }
+    return Network("chp", list(range(T)), {}, tables)
+
+
+@pytest.mark.parametrize("efficiency2", [[0.5], [0.5, 0.6]])
+def test_a_multi_port_link_delivers_at_every_port(efficiency2):
+    """Topology.portsOf/portEfficiency: bus2 receives efficiency2 x p0 (a
+    series over the static value); a link leaving bus2 empty has two ports."""
+    from oracle import oracle as O
+    n = _chp_network(efficiency2)
+    model = lopf.build(n)
+    res = lopf.LopfResult(n, model, O.solve(model.problem, X.PARAMS))
+    assert res.status.name == "OPTIMAL"
+    for t, e2 in enumerate(efficiency2):
+        assert res.dispatch("Link", "chp", t) == pytest.approx(100.0, abs=1e-5)   # 40 MW of power at 0.4
+        assert res.dispatch("Link", "boiler", t) == pytest.approx(0.0, abs=1e-5)
+        assert res.dispatch("Generator", "dump", t) == pytest.approx(30.0 - 100.0 * e2, abs=1e-5)
+    assert res.objective == pytest.approx(2000.0 * len(efficiency2), rel=1e-8)
+
+
+def test_a_link_port_on_an_unknown_bus_is_refused():
+    n = _chp_network([0.5])
+    n.table("Link").static["bus2"]["chp"] = "steam"
+    with pytest.raises(lopf.UnsupportedNetwork, match="steam"):
+        lopf.build(n)
