@@ -113,7 +113,47 @@ class LopfResult:
         return self.objective + self.model.objective_constant
 
     def dispatch(self, component: str, entity: str, t: int) -> float:
-        return float(self.solution.primal[self.model.columns[(component, entity, t)]])
+        """A column's value; for a StorageUnit the net injection p_dispatch -
+        p_store (PyPSA's storage_units_t.p), for a Store its signed power."""
+        if component == "StorageUnit":
+            return self.discharging(entity, t) - self.charging(entity, t)
+        if component == "Store":
+            return self._col("Store-p", entity, t)
+        return self._col(component, entity, t)
+
+    def _col(self, key: str, entity: str, t: int) -> float:
+        return float(self.solution.primal[self.model.columns[(key, entity, t)]])
+
+    def energy(self, entity: str, t: int) -> float:
+        """A store's energy at the end of snapshot t."""
+        return self._col("Store-e", entity, t)
+
+    def state_of_charge(self, entity: str, t: int) -> float:
+        """A storage unit's state of charge at the end of snapshot t."""
+        return self._col("StorageUnit-state_of_charge", entity, t)
+
+    def charging(self, entity: str, t: int) -> float:
+        return self._col("StorageUnit-p_store", entity, t)
+
+    def discharging(self, entity: str, t: int) -> float:
+        return self._col("StorageUnit-p_dispatch", entity, t)
+
+    def spill(self, entity: str, t: int) -> float:
+        return self._col("StorageUnit-spill", entity, t)
+
+    def marginal_price(self, bus: str, t: int) -> float:
+        """The dual of the bus's balance row at snapshot t, through the row
+        translation (so the sign is the constraint's as written), per unit of
+        the snapshot's objective weighting (``LopfResult.marginalPrice``,
+        Lopf.scala:692-706)."""
+        if (bus, t) not in self.model.balance_rows:
+            raise KeyError(f"no balance row for bus '{bus}' at snapshot {t}")
+        duals = self.__dict__.get("_duals")
+        if duals is None:
+            duals = self.model.translation.original_duals(self.solution.dual)
+            self.__dict__["_duals"] = duals
+        return float(duals[self.model.balance_rows[(bus, t)]]) / (self.model.network or self.network).weighting(
+            "objective", t)
 
     def capacity(self, component: str, entity: str) -> float:
         """The chosen capacity of an extendable entity, else its given one

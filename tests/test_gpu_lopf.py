@@ -43,3 +43,31 @@ def test_scigrid_de_on_the_device_at_1e_6(mixed):
         X.check_scigrid(lambda p, q: cuda.mixed_solve(p, q).solution, params, 1e-5)
     else:
         X.check_scigrid(lambda p, q: cuda.solve(p, q, precision=64), params, 1e-5)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_prices_from_the_device(mixed):
+    """Nodal prices (balance-row duals) from the device solve: every interior
+    zero-emission generator is priced at its marginal cost."""
+    import numpy as np
+    from noaidi_b200.network import lopf
+    from noaidi_b200.prima import cuda
+    n = X.network("ac-dc-dispatch")
+    model = lopf.build(n)
+    sol = cuda.mixed_solve(model.problem, X.PARAMS).solution if mixed else \
+        cuda.solve(model.problem, X.PARAMS, precision=64)
+    res = lopf.LopfResult(n, model, sol)
+    gens, carriers = n.table("Generator"), n.table("Carrier")
+    checked = 0
+    for t in range(len(n.snapshots)):
+        for g in gens.ids:
+            p_nom = float(gens.value("p_nom", g))
+            lo, hi = p_nom * gens.at("p_min_pu", g, t), p_nom * gens.at("p_max_pu", g, t)
+            p = res.dispatch("Generator", g, t)
+            carrier = str(gens.value("carrier", g))
+            if float(carriers.value("co2_emissions", carrier)) == 0.0 and lo + 1e-2 < p < hi - 1e-2:
+                checked += 1
+                assert res.marginal_price(str(gens.value("bus", g)), t) == pytest.approx(
+                    gens.at("marginal_cost", g, t), abs=1e-3)
+    assert checked >= 2
+    assert all(np.isfinite(res.marginal_price(b, t)) for b in n.table("Bus").ids for t in range(len(n.snapshots)))

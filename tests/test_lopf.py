@@ -280,3 +280,54 @@ def test_a_link_port_on_an_unknown_bus_is_refused():
     n.table("Link").static["bus2"]["chp"] = "steam"
     with pytest.raises(lopf.UnsupportedNetwork, match="steam"):
         lopf.build(n)
+
+
+def test_prices_are_duals_that_close_the_gap():
+    """LopfSuite.scala:620-655: the dual side is a real optimum (strong
+    duality) and every nodal price is finite."""
+    from oracle import oracle as O
+    n = X.network("ac-dc-dispatch")
+    model = lopf.build(n)
+    res = lopf.LopfResult(n, model, O.solve(model.problem, X.PARAMS))
+    sol = res.solution
+    assert sol.objective_value == pytest.approx(sol.dual_objective_value, abs=1e-6 * max(1.0, abs(sol.objective_value)))
+    for bus in n.table("Bus").ids:
+        for t in range(len(n.snapshots)):
+            assert np.isfinite(res.marginal_price(bus, t))
+
+
+def test_an_interior_clean_generator_sets_its_bus_price():
+    """LopfSuite.scala:713-747: a zero-emission generator strictly inside
+    its limits is marginal, so its bus price equals its marginal cost."""
+    from oracle import oracle as O
+    n = X.network("ac-dc-dispatch")
+    model = lopf.build(n)
+    res = lopf.LopfResult(n, model, O.solve(model.problem, X.PARAMS))
+    gens, carriers = n.table("Generator"), n.table("Carrier")
+    checked = 0
+    for t in range(len(n.snapshots)):
+        for g in gens.ids:
+            p_nom = float(gens.value("p_nom", g))
+            lo, hi = p_nom * gens.at("p_min_pu", g, t), p_nom * gens.at("p_max_pu", g, t)
+            p = res.dispatch("Generator", g, t)
+            carrier = str(gens.value("carrier", g))
+            clean = carrier in carriers.ids and float(carriers.value("co2_emissions", carrier)) == 0.0
+            if clean and lo + 1e-2 < p < hi - 1e-2:
+                checked += 1
+                assert res.marginal_price(str(gens.value("bus", g)), t) == pytest.approx(
+                    gens.at("marginal_cost", g, t), abs=1e-3), (t, g)
+    assert checked >= 2
+
+
+def test_storage_accessors_follow_pypsas_conventions():
+    from oracle import oracle as O
+    n = X.network("storage-cycle")
+    exp = X.expected("storage-cycle")
+    model = lopf.build(n)
+    res = lopf.LopfResult(n, model, O.solve(model.problem, X.PARAMS))
+    for u in n.table("StorageUnit").ids:
+        for t in range(len(n.snapshots)):
+            assert res.dispatch("StorageUnit", u, t) == pytest.approx(res.discharging(u, t) - res.charging(u, t))
+            assert res.state_of_charge(u, t) == pytest.approx(
+                X.frame_value(exp["storage_state_of_charge"], t, u), abs=1e-3)
+            assert res.spill(u, t) == pytest.approx(X.frame_value(exp["storage_spill"], t, u), abs=1e-3)
