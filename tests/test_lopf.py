@@ -331,3 +331,88 @@ def test_storage_accessors_follow_pypsas_conventions():
             assert res.state_of_charge(u, t) == pytest.approx(
                 X.frame_value(exp["storage_state_of_charge"], t, u), abs=1e-3)
             assert res.spill(u, t) == pytest.approx(X.frame_value(exp["storage_spill"], t, u), abs=1e-3)
+
+
+@pytest.mark.parametrize("name", ["ac-dc-meshed", "storage-hvdc"])
+def test_base_rows_stay_one_for_one_under_expansion(name):
+    """SclopfSuite.scala:538-555: every equality block is emitted before the
+    first inequality, so original row r is standard-form row r."""
+    from noaidi_b200.prima.model import Direct, Negated
+    model = lopf.build(X.network(name))
+    t = model.translation
+    for r in range(t.num_original_rows):
+        e = t.expansion_of(r)
+        assert isinstance(e, (Direct, Negated)) and e.row == r, (r, e)
+
+
+def test_every_post_contingency_flow_stays_within_its_rating():
+    """SclopfSuite.scala:128-157: each post-outage flow rebuilt from the
+    solved flows and the factors respects the rating."""
+    from oracle import oracle as O
+    n = X.network("sclopf-triangle")
+    outages = X.expected("sclopf-triangle")["sclopf"]["branch_outages"]
+    model = lopf.build_sclopf(n, outages)
+    res = lopf.LopfResult(n, model, O.solve(model.problem, X.PARAMS))
+    [(carrier, buses, branches)] = lopf.sub_networks(n)
+    names, factors, _ = lopf.lodf(n, carrier, buses, branches)
+    lines = n.table("Line")
+    checked = 0
+    for t in range(len(n.snapshots)):
+        for j, (_, o) in enumerate(names):
+            for k, (_, l) in enumerate(names):
+                if k == j:
+                    continue
+                after = res.dispatch("Line", l, t) + factors[k, j] * res.dispatch("Line", o, t)
+                assert abs(after) <= float(lines.value("s_nom", l)) + 1e-3, (t, o, l, after)
+                checked += 1
+    assert checked >= 12
+
+
+def test_no_security_rows_cross_a_sub_network_boundary():
+    """SclopfSuite.scala:240-272: two islands; outaging one triangle line adds
+    rows for the other two triangle lines only."""
+    from noaidi_b200.network.pypsa_csv import Network, Table
+    lines = {"AB": ("A", "B"), "BC": ("B", "C"), "AC": ("A", "C"), "XY1": ("X", "Y"), "XY2": ("X", "Y")}
+    n = Network("split", [0], {}, {
+        "Bus": Table("Bus", list("ABCXY"), {"v_nom": dict.fromkeys("ABCXY", 380.0)}),
+        "Line": Table("Line", list(lines), {"bus0": {k: v[0] for k, v in lines.items()},
+                                            "bus1": {k: v[1] for k, v in lines.items()},
+                                            "x": dict.fromkeys(lines, 0.1), "s_nom": dict.fromkeys(lines, 150.0)}),
+        "Generator": Table("Generator", ["g1", "g2"], {"bus": {"g1": "A", "g2": "X"},
+                                                       "p_nom": {"g1": 400.0, "g2": 400.0},
+                                                       "marginal_cost": {"g1": 10.0, "g2": 10.0}}),
+        "Load": Table("Load", ["l1", "l2"], {"bus": {"l1": "C", "l2": "Y"}, "p_set": {"l1": 100.0, "l2": 100.0}}),
+    })
+    assert len(lopf.sub_networks(n)) == 2
+    base = lopf.build(n).problem.num_constraints
+    one = lopf.build_sclopf(n, [("Line", "AB")])
+    assert one.problem.num_constraints - base == 4  # two two-sided rows
+
+
+def test_sclopf_under_an_emissions_cap_keeps_the_caps_sign():
+    """SclopfSuite.scala:274-310: a network with a CO2 cap builds security
+    rows, and the cap stays a negated (<=) row through the rebuild."""
+    from noaidi_b200.prima.model import Negated
+    n = X.network("ac-dc-co2")
+    base = lopf.build(n)
+    secure = lopf.build_sclopf(n, ["0", "1", "5"])
+    assert secure.problem.num_constraints > base.problem.num_constraints
+    count = lambda t, k: sum(isinstance(t.expansion_of(r), Negated) for r in range(k))
+    k = base.translation.num_original_rows
+    assert count(base.translation, k) > 0
+    assert count(secure.translation, k) == count(base.translation, k)
+
+
+def test_extendable_generation_alone_is_allowed_under_security():
+    """SclopfSuite.scala:440-500: with the lines fixed, an expansion network
+    builds security rows and the secure optimum costs at least the plain one."""
+    from oracle import oracle as O
+    n = X.network("ac-dc-meshed")
+    lines = n.table("Line")
+    lines.static["s_nom_extendable"] = dict.fromkeys(lines.ids, False)
+    plain, secure = lopf.build(n), lopf.build_sclopf(n, ["0", "1", "5"])
+    assert secure.problem.num_constraints > plain.problem.num_constraints
+    params = X.PARAMS.copy(eps_abs=1e-7, eps_rel=1e-7)
+    a, b = O.solve(plain.problem, params), O.solve(secure.problem, params)
+    assert a.status.name == b.status.name == "OPTIMAL"
+    assert b.objective_value >= a.objective_value - 1e-6 * abs(a.objective_value)
