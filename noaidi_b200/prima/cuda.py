@@ -6,7 +6,8 @@
   iteration on the device (one persistent launch).
 * :func:`mixed_solve` -- ``MixedPrecision.solve`` (``MixedPrecision.scala:104-199``)
   with both passes on the device.
-* :func:`solve_batch` -- ``PrimaZio.solveAll``'s shape in one launch.
+* :func:`solve_batch` -- ``PrimaZio.solveAll``'s shape in one launch, and
+  :func:`solve_labelled` -- ``solveLabelled``'s.
 
 There is no CPU fallback: if the library is missing or no sm_100 device is
 present these raise.
@@ -541,6 +542,14 @@ class DeviceProblem:
         if self.handle is not None and not self.ctx._closed:
             _check(self.ctx.lib.prima_problem_free(self.ctx.handle, self.handle))
         self.handle = None
+
+
+def solve_labelled(labelled: Sequence[tuple], params: PdhgParams = PdhgParams(), **kw) -> list[tuple]:
+    """``PrimaZio.solveLabelled`` (PrimaZio.scala:68-76): every (label,
+    problem) solved in one device launch, each result kept with its label,
+    in order."""
+    labels = [label for label, _ in labelled]
+    return list(zip(labels, solve_batch([p for _, p in labelled], params, **kw)))
 
 
 def solve_batch(problems: Sequence[LpProblem], params: PdhgParams = PdhgParams(), precision: int = 64,

@@ -77,3 +77,25 @@ def test_mixed_batch_matches_single_mixed_solves(scheme):
             conv = convergence(got.solution.kkt, float(np.linalg.norm(prob.rhs)),
                                float(np.linalg.norm(prob.objective)), 1e-9, 1e-9)
             assert conv.converged
+
+
+def test_labelled_results_keep_their_labels():
+    """PrimaZioSuite.scala:73-80: solveLabelled returns each result with its
+    label, in the order given."""
+    items = [("dispatch", F.economic_dispatch().problem), ("mix", F.product_mix().problem)]
+    got = cuda().solve_labelled(items, P9)
+    assert [label for label, _ in got] == ["dispatch", "mix"]
+    for (label, sol), (_, p) in zip(got, items):
+        ref = O.solve(p, P9)
+        assert sol.status == SolveStatus.OPTIMAL
+        assert sol.objective_value == pytest.approx(ref.objective_value, rel=1e-8)
+
+
+def test_a_raised_cancel_flag_interrupts_every_instance():
+    """PrimaZioSuite.scala:40-58: an interrupted sweep stops at the next
+    evaluation point of every instance, reporting Interrupted."""
+    import ctypes
+    flag = ctypes.c_int32(1)
+    insts = [F.random_feasible(5 + k, 200, 40, 80) for k in range(3)]
+    got = cuda().solve_batch(insts, PdhgParams(eps_abs=1e-16, eps_rel=1e-16), cancel=flag)
+    assert all(s.status == SolveStatus.INTERRUPTED and s.iterations == 64 for s in got), got
