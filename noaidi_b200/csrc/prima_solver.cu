@@ -210,6 +210,7 @@ struct HotShared {
   int2 tiles[2 * kHotBatch];       // per tile of the batch: (first row, first nonzero) of it and of the next
   int issued;                      // tiles of the batch issued so far
   int flag;
+  int primed;                      // the next hot phase's first stages are already issued
 };
 
 // The tile engine over a table of ntiles tiles (see above).  rp == nullptr:
@@ -218,6 +219,69 @@ struct HotShared {
 // index-order sum from zero, as csr_tiles), slices the tile's vector slices
 // (stride kHotRows).  Returns false, uniformly over the block, when the
 // team's abort flag is up.
+// Issue tile j of the batch staged in hs.tiles into stage j % kStages: its
+// vector slices and, for an SpMV, its row pointers, column indices and
+// values, all completing on the stage's mbarrier.  One thread.
+template <typename T>
+__device__ __forceinline__ void issue_tile(int j, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                                           const T *__restrict__ v, const T *const *vecs, int nv, unsigned char *smem,
+                                           HotShared &hs) {
+  using L = HotLayout<T>;
+  constexpr int S = L::kStages;
+  const int b = j % S;
+  unsigned char *buf = smem + b * L::stage_bytes;
+  const int2 e0 = hs.tiles[2 * j], e1 = hs.tiles[2 * j + 1];
+  const int32_t r0 = e0.x, rows = e1.x - e0.x;
+  const unsigned vb = ((unsigned)rows * (unsigned)sizeof(T) + 15u) & ~15u;
+  unsigned total = (unsigned)nv * vb, rpb = 0, cb = 0, vvb = 0;
+  int32_t ka = 0;
+  if (rp) {
+    rpb = ((unsigned)(rows + 1) * 4u + 15u) & ~15u;
+    ka = e0.y & ~3;
+    const int32_t kbnd = (e1.y + 3) & ~3;
+    if (kbnd - ka <= L::kCap && kbnd > ka) {
+      cb = (unsigned)(kbnd - ka) * 4u;
+      vvb = (unsigned)(kbnd - ka) * (unsigned)sizeof(T);
+    }
+    total += rpb + cb + vvb;
+  }
+  fence_proxy_async();
+  hs.issued = j + 1;
+  mbar_expect_tx(&hs.bars[b], total);
+  for (int i = 0; i < nv; i++) bulk_copy(buf + L::vec_off + i * L::vec_stride, vecs[i] + r0, vb, &hs.bars[b]);
+  if (rp) {
+    bulk_copy(buf, rp + r0, rpb, &hs.bars[b]);
+    if (cb) {
+      bulk_copy(buf + L::ci_off, ci + ka, cb, &hs.bars[b]);
+      bulk_copy(buf + L::v_off, v + ka, vvb, &hs.bars[b]);
+    }
+  }
+}
+
+// One warp stages this block's first batch of tiles and issues its first
+// stages, ahead of the hot phase that will consume them (hs.primed tells it
+// to start from there).  The stages and the tile list must be free.
+template <typename T>
+__device__ __forceinline__ void prime_tiles(int32_t ntiles, int nb, int rank, const int2 *__restrict__ table,
+                                            const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                                            const T *__restrict__ v, const T *const *vecs, int nv,
+                                            unsigned char *smem, HotShared &hs) {
+  constexpr int S = HotLayout<T>::kStages;
+  const int lane = threadIdx.x & 31;
+  const int32_t mine = rank < ntiles ? (ntiles - rank + nb - 1) / nb : 0;
+  if (mine == 0) return;
+  const int nj = min(kHotBatch, mine);
+  for (int e = lane; e < 2 * nj; e += 32) hs.tiles[e] = __ldg(table + rank + (int64_t)(e >> 1) * nb + (e & 1));
+  __syncwarp();
+  if (lane == 0) {
+    for (int b = 0; b < S; b++) hs.done[b] = 0;
+    hs.issued = 0;
+    for (int j = 0; j < S && j < nj; j++) issue_tile<T>(j, rp, ci, v, vecs, nv, smem, hs);
+    hs.primed = 1;
+  }
+  __syncwarp();
+}
+
 template <typename T, typename Epi>
 __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, const int2 *__restrict__ table,
                                           const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
@@ -229,48 +293,27 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
   const bool spmv = rp != nullptr;
   const int lane = threadIdx.x & 31;
   const int32_t mine = rank < ntiles ? (ntiles - rank + nb - 1) / nb : 0;  // this block's tiles
+  const bool primed = hs.primed != 0;  // the first batch is staged and its first stages issued
   for (int32_t jb = 0; jb < mine; jb += kHotBatch) {
     const int nj = min(kHotBatch, mine - jb);
-    for (int e = threadIdx.x; e < 2 * nj; e += kThreads) {
-      const int64_t t = rank + (int64_t)(jb + (e >> 1)) * nb + (e & 1);
-      hs.tiles[e] = __ldg(table + t);
+    const bool pre = primed && jb == 0;
+    if (!pre) {
+      for (int e = threadIdx.x; e < 2 * nj; e += kThreads) {
+        const int64_t t = rank + (int64_t)(jb + (e >> 1)) * nb + (e & 1);
+        hs.tiles[e] = __ldg(table + t);
+      }
+      if (threadIdx.x < S) hs.done[threadIdx.x] = 0;
+      if (threadIdx.x == 0) hs.issued = 0;
+      __syncthreads();
     }
-    if (threadIdx.x < S) hs.done[threadIdx.x] = 0;
-    if (threadIdx.x == 0) hs.issued = 0;
-    __syncthreads();
     auto issue = [&](int j) {  // one thread
-      const int b = j % S;
-      unsigned char *buf = smem + b * L::stage_bytes;
-      const int2 e0 = hs.tiles[2 * j], e1 = hs.tiles[2 * j + 1];
-      const int32_t r0 = e0.x, rows = e1.x - e0.x;
-      const unsigned vb = ((unsigned)rows * (unsigned)sizeof(T) + 15u) & ~15u;
-      unsigned total = (unsigned)nv * vb, rpb = 0, cb = 0, vvb = 0;
-      int32_t ka = 0;
-      if (spmv) {
-        rpb = ((unsigned)(rows + 1) * 4u + 15u) & ~15u;
-        ka = e0.y & ~3;
-        const int32_t kbnd = (e1.y + 3) & ~3;
-        if (kbnd - ka <= L::kCap && kbnd > ka) {
-          cb = (unsigned)(kbnd - ka) * 4u;
-          vvb = (unsigned)(kbnd - ka) * (unsigned)sizeof(T);
-        }
-        total += rpb + cb + vvb;
-      }
-      fence_proxy_async();
-      hs.issued = j + 1;
-      mbar_expect_tx(&hs.bars[b], total);
-      for (int i = 0; i < nv; i++) bulk_copy(buf + L::vec_off + i * L::vec_stride, vecs[i] + r0, vb, &hs.bars[b]);
-      if (spmv) {
-        bulk_copy(buf, rp + r0, rpb, &hs.bars[b]);
-        if (cb) {
-          bulk_copy(buf + L::ci_off, ci + ka, cb, &hs.bars[b]);
-          bulk_copy(buf + L::v_off, v + ka, vvb, &hs.bars[b]);
-        }
-      }
+      issue_tile<T>(j, rp, ci, v, vecs, nv, smem, hs);
     };
-    if (threadIdx.x == 0)
-      for (int j = 0; j < S && j < nj; j++) issue(j);
-    __syncthreads();
+    if (!pre) {
+      if (threadIdx.x == 0)
+        for (int j = 0; j < S && j < nj; j++) issue(j);
+      __syncthreads();
+    }
     int j = 0;
     for (; j < nj; j++) {
       const int b = j % S;
@@ -416,6 +459,10 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
     }
     __syncthreads();
     if (hs.flag) return false;
+  }
+  if (primed) {
+    __syncthreads();  // every thread has read the flag
+    if (threadIdx.x == 0) hs.primed = 0;
   }
   return true;
 }
@@ -831,6 +878,22 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
   return ok;
 }
 
+// The vectors phase B stages per tile, in slice order: y, kx, q, then the
+// running sums when a commit is pending, then the anchored lower bound.
+// None of them changes during phase A, so they can be staged before it ends.
+template <typename T>
+__device__ __forceinline__ int b_operands(const Args<T> &a, const Control &s, const T *(&vecs)[6]) {
+  vecs[0] = a.y[s.yc];
+  vecs[1] = a.kx[s.kxc];
+  vecs[2] = a.q;
+  vecs[3] = a.sy;
+  vecs[4] = a.skx;
+  vecs[5] = a.ylo;
+  int nv = s.pend ? 5 : 3;
+  if (a.ylo) vecs[nv++] = a.ylo;
+  return nv;
+}
+
 // Dual half of a trial: K xbar, dualStep, the speculative kx commit value;
 // operands streamed by TMA.
 template <typename T>
@@ -838,19 +901,12 @@ __device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsi
                         unsigned &par) {
   double v[2] = {0.0, 0.0};
   const T sigma = (T)s.sigma, w = (T)s.pend_w;
-  const T *y = a.y[s.yc];
-  const T *kx = a.kx[s.kxc];
   T *y_out = a.y[s.yc ^ 1];
   T *kx_out = a.kx[s.kxc ^ 1];
   const bool pend = s.pend != 0;
-  const T *vecs[6] = {y, kx, a.q, a.sy, a.skx, a.ylo};
-  int nv = 3;
-  if (pend) nv = 5;
-  const int iylo = nv;
-  if (a.ylo) {
-    vecs[nv] = a.ylo;
-    nv++;
-  }
+  const T *vecs[6];
+  const int nv = b_operands(a, s, vecs);
+  const int iylo = pend ? 5 : 3;
   const bool has_lo = a.ylo != nullptr;
   const bool ok = hot_tiles<T>(a.ntiles_k, tm.nb, tm.rank, a.tiles_k, a.kp, a.kci, a.kv, (const T *)a.xbar, vecs, nv, smem, hs, par,
                                &a.sync->abort, [&](int32_t r, int i, T kb, const T *sl) {
@@ -1273,7 +1329,17 @@ __device__ __forceinline__ void load_control(const Args<T> &a, Control &snap) {
 // leaves; the host reports PRIMA_ERR_TIMEOUT.  A one-block team synchronises
 // with __syncthreads and keeps its Control in shared memory.
 template <typename T>
-__device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const Team &tm) {
+__device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const Team &tm, unsigned char *smem,
+                               HotShared &hs, unsigned &par) {
+  // After phase A comes phase B, whose tiles and vectors are already final:
+  // one warp stages its first tiles while the block waits for the release
+  // (the last block, right after releasing the others).
+  const bool prime = phase == PH_A && tm.nb > 1;
+  auto prime_b = [&] {
+    const T *vecs[6];
+    const int nv = b_operands(a, snap, vecs);
+    prime_tiles<T>(a.ntiles_k, tm.nb, tm.rank, a.tiles_k, a.kp, a.kci, a.kv, vecs, nv, smem, hs);
+  };
   __shared__ int s_last, s_ok;
   __shared__ double s_red[kMaxQ];
   if (tm.nb == 1) {
@@ -1350,7 +1416,11 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
       __threadfence();
       st_release(&a.sync->gen, s_gen + 1);
       s_gen += 1;
+    } else if (prime && threadIdx.x >> 5 == 1) {
+      prime_b();
     }
+  } else if (prime && threadIdx.x >> 5 == 1) {
+    prime_b();
   } else if (threadIdx.x == 0) {
     unsigned long long spins = 0;
     while (ld_acquire(&a.sync->gen) == s_gen) {
@@ -1369,6 +1439,14 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     if (phase == PH_A) snap.phase = PH_B;
   }
   __syncthreads();
+  if (!s_ok && hs.primed && threadIdx.x == 0) {  // leaving: let the staged copies land first (bounded)
+    constexpr int S = HotLayout<T>::kStages;
+    for (int u = 0; u < hs.issued; u++) {
+      mbar_wait(&hs.bars[u % S], (par >> (u % S)) & 1u);
+      par ^= 1u << (u % S);
+    }
+    hs.primed = 0;
+  }
   if (s_ok && phase != PH_A) load_control(a, snap);
   return s_ok;
 }
@@ -1397,7 +1475,7 @@ __device__ __forceinline__ bool run_solve(const Args<T> &a, const Team &tm, Cont
       default: break;
     }
     (void)ok;  // a failed tile wait has raised the team's abort flag; the barrier sees it
-    if (!barrier_decide(a, snap, ph, tm)) {
+    if (!barrier_decide(a, snap, ph, tm, s_dyn, hs, par)) {
       alive = false;
       break;
     }
@@ -1410,6 +1488,7 @@ __device__ __forceinline__ void init_stages(HotShared &hs) {
   if (threadIdx.x == 0) {
     for (int i = 0; i < kMaxStages; i++) mbar_init(&hs.bars[i], 1);
     fence_mbar_init();
+    hs.primed = 0;
   }
   __syncthreads();
 }
