@@ -465,7 +465,7 @@ def main():
 # DRAM bytes (read + write) per step-size trial of pdhg_kernel<float> on this
 # workload, from an ncu capture of a bounded run of the same instance; None
 # until measured.
-TRAFFIC_BYTES_PER_TRIAL = 141.1e6
+TRAFFIC_BYTES_PER_TRIAL = 140.5e6
 
 if __name__ == "__main__":
     main()
