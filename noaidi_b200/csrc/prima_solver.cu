@@ -211,6 +211,7 @@ struct HotShared {
   int issued;                      // tiles of the batch issued so far
   int flag;
   int primed;                      // the next hot phase's first stages are already issued
+  const int2 *listed;              // the table whose first batch hs.tiles holds, else nullptr
 };
 
 // The tile engine over a table of ntiles tiles (see above).  rp == nullptr:
@@ -274,11 +275,25 @@ __device__ __forceinline__ void prime_tiles(int32_t ntiles, int nb, int rank, co
   for (int e = lane; e < 2 * nj; e += 32) hs.tiles[e] = __ldg(table + rank + (int64_t)(e >> 1) * nb + (e & 1));
   __syncwarp();
   if (lane == 0) {
+    hs.listed = table;
     for (int b = 0; b < S; b++) hs.done[b] = 0;
     hs.issued = 0;
     for (int j = 0; j < S && j < nj; j++) issue_tile<T>(j, rp, ci, v, vecs, nv, smem, hs);
     hs.primed = 1;
   }
+  __syncwarp();
+}
+
+// One warp stages this block's first batch of tiles of a table in hs.tiles
+// (no copies issued), for the next hot phase over it to skip that load.
+__device__ __forceinline__ void list_tiles(int32_t ntiles, int nb, int rank, const int2 *__restrict__ table,
+                                           HotShared &hs) {
+  const int lane = threadIdx.x & 31;
+  const int32_t mine = rank < ntiles ? (ntiles - rank + nb - 1) / nb : 0;
+  const int nj = min(kHotBatch, mine);
+  for (int e = lane; e < 2 * nj; e += 32) hs.tiles[e] = __ldg(table + rank + (int64_t)(e >> 1) * nb + (e & 1));
+  __syncwarp();
+  if (lane == 0) hs.listed = table;
   __syncwarp();
 }
 
@@ -298,12 +313,17 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
     const int nj = min(kHotBatch, mine - jb);
     const bool pre = primed && jb == 0;
     if (!pre) {
-      for (int e = threadIdx.x; e < 2 * nj; e += kThreads) {
-        const int64_t t = rank + (int64_t)(jb + (e >> 1)) * nb + (e & 1);
-        hs.tiles[e] = __ldg(table + t);
-      }
+      if (!(jb == 0 && hs.listed == table))  // the first batch may already be staged
+        for (int e = threadIdx.x; e < 2 * nj; e += kThreads) {
+          const int64_t t = rank + (int64_t)(jb + (e >> 1)) * nb + (e & 1);
+          hs.tiles[e] = __ldg(table + t);
+        }
+      __syncthreads();  // every thread has read hs.listed
       if (threadIdx.x < S) hs.done[threadIdx.x] = 0;
-      if (threadIdx.x == 0) hs.issued = 0;
+      if (threadIdx.x == 0) {
+        hs.issued = 0;
+        hs.listed = jb == 0 ? table : nullptr;
+      }
       __syncthreads();
     }
     auto issue = [&](int j) {  // one thread
@@ -1335,6 +1355,9 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
   // one warp stages its first tiles while the block waits for the release
   // (the last block, right after releasing the others).
   const bool prime = phase == PH_A && tm.nb > 1;
+  // After phase B comes phase A (or a checkpoint first, which leaves the
+  // list alone): its tile list is static, so stage that too while waiting.
+  const bool list_a = phase == PH_B && tm.nb > 1;
   auto prime_b = [&] {
     const T *vecs[6];
     const int nv = b_operands(a, snap, vecs);
@@ -1418,9 +1441,13 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
       s_gen += 1;
     } else if (prime && threadIdx.x >> 5 == 1) {
       prime_b();
+    } else if (list_a && threadIdx.x >> 5 == 1) {
+      list_tiles(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, hs);
     }
   } else if (prime && threadIdx.x >> 5 == 1) {
     prime_b();
+  } else if (list_a && threadIdx.x >> 5 == 1) {
+    list_tiles(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, hs);
   } else if (threadIdx.x == 0) {
     unsigned long long spins = 0;
     while (ld_acquire(&a.sync->gen) == s_gen) {
@@ -1489,6 +1516,7 @@ __device__ __forceinline__ void init_stages(HotShared &hs) {
     for (int i = 0; i < kMaxStages; i++) mbar_init(&hs.bars[i], 1);
     fence_mbar_init();
     hs.primed = 0;
+    hs.listed = nullptr;
   }
   __syncthreads();
 }
