@@ -27,8 +27,6 @@ import math
 from dataclasses import dataclass
 from typing import Optional
 
-import numpy as np
-
 from ..prima.bnb import BnbParams, MilpSolution, MilpStatus, NodeSolver, device_node_solver, solve_with
 from ..prima.model import LpBuilder, LpProblem
 from ..prima.types import PdhgParams

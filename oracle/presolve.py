@@ -27,7 +27,7 @@ one holding the column, by moving the column's reduced cost onto the row
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass, replace
+from dataclasses import replace
 from typing import Optional
 
 import numpy as np
