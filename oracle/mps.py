@@ -1,7 +1,7 @@
 """A Python restatement of ``MpsReader``
 (modules/prima-mps/src/main/scala/org/noaidi/prima/mps/MpsReader.scala).
 
-TEST INFRASTRUCTURE ONLY: the checker for the product's C++ reader
+TEST INFRASTRUCTURE ONLY: the oracle for the product's C++ reader
 (``prima_mps_read`` in libprima_cuda.so, wrapped by noaidi_b200/prima/mps.py).
 Imported by ``tests/`` only.
 

@@ -1,8 +1,8 @@
 """ctypes loader for the C restatement of Prima's PDHG path.
 
 TEST INFRASTRUCTURE ONLY.  Imported by ``tests/``, ``__graft_entry__.smoke()``
-and ``bench.py``'s CPU-baseline leg, and there only as the checker / the
-timed CPU reference.  The product (``noaidi_b200``) never imports this.
+and ``bench.py``'s CPU-baseline leg, and there only as the oracle results
+are compared with, or as the timed CPU reference.  The product (``noaidi_b200``) never imports this.
 """
 from __future__ import annotations
 

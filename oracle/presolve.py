@@ -1,7 +1,7 @@
 """A Python restatement of ``Presolve``
 (modules/prima-core/src/main/scala/org/noaidi/prima/Presolve.scala).
 
-TEST INFRASTRUCTURE ONLY: the checker for the product's C++ presolve
+TEST INFRASTRUCTURE ONLY: the oracle for the product's C++ presolve
 (``prima_presolve`` in libprima_cuda.so, wrapped by
 noaidi_b200/prima/presolve.py).  Imported by ``tests/`` only.
 

@@ -1,7 +1,7 @@
 """MILP fixtures of BranchAndBoundSuite (modules/prima-core/src/test/scala/
 org/noaidi/prima/BranchAndBoundSuite.scala), each with a fractional
 relaxation and an optimum worked out by hand, and an oracle node solver:
-the reference's FP64 PDHG restated in C, used here only as the checker."""
+the reference's FP64 PDHG restated in C, used here only as the oracle."""
 import numpy as np
 
 from noaidi_b200.prima import LpProblem, PdhgParams
