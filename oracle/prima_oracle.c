@@ -1,6 +1,6 @@
 /*
  * CPU restatement of Prima's restarted-PDHG path.  TEST INFRASTRUCTURE ONLY:
- * the parity checker for libprima_cuda.so and the timed CPU baseline.
+ * the parity oracle for libprima_cuda.so and the timed CPU baseline.
  *
  * Every function follows one reference function and cites it (paths are
  * relative to the oluies/noaidi repository; "core/" abbreviates

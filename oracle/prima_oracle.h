@@ -1,6 +1,6 @@
 /*
  * CPU restatement of Prima's restarted-PDHG path (oluies/noaidi, module
- * prima-core).  TEST INFRASTRUCTURE ONLY: this library is the parity checker
+ * prima-core).  TEST INFRASTRUCTURE ONLY: this library is the parity oracle
  * for libprima_cuda.so and the timed CPU baseline.  Nothing in the product
  * links it.
  *
