@@ -37,6 +37,10 @@ int32_t DeviceBuffer::reserve(size_t b) {
   if (b == 0) b = 256;
   cudaError_t e = cudaMalloc(&ptr, b + 64);
   if (e != cudaSuccess) {
+    // The failure is reported here; take it off the thread's last-error slot,
+    // where the next launch check would otherwise find it and blame that
+    // launch.
+    (void)cudaGetLastError();
     ptr = nullptr;
     set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? PRIMA_ERR_OUT_OF_MEMORY : PRIMA_ERR_CUDA;

@@ -198,3 +198,22 @@ def test_long_rows_take_the_warp_path_and_match_the_oracle():
         got = gpu_solve(P, p, precision=prec)
         assert got.status == ref.status == SolveStatus.OPTIMAL
         assert F.relative_gap(got.objective_value, ref.objective_value) <= (1e-6 if prec == 64 else 1e-4)
+
+
+def test_an_allocation_the_device_cannot_hold_fails_cleanly():
+    """Fault injection on the host side: a 1 TiB vector cannot be allocated,
+    which answers PRIMA_ERR_OUT_OF_MEMORY, and the context stays usable --
+    the next operations and a whole solve succeed."""
+    from noaidi_b200.prima import cuda
+    ctx = cuda.Context(0, 64)
+    try:
+        h = ctypes.c_int64()
+        assert ctx.lib.prima_vec_alloc(ctx.handle, 1 << 37, ctypes.byref(h)) == cuda.ERR_OUT_OF_MEMORY
+        assert b"cudaMalloc" in ctx.lib.prima_last_error()
+        ok = ctypes.c_int64()
+        assert ctx.lib.prima_vec_alloc(ctx.handle, 1000, ctypes.byref(ok)) == cuda.OK
+        p = F.economic_dispatch().problem
+        s = cuda.solve(p, P9, ctx=ctx)
+        assert s.status == SolveStatus.OPTIMAL and s.objective_value == pytest.approx(3700.0, rel=1e-8)
+    finally:
+        ctx.close()
