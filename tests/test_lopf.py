@@ -416,3 +416,44 @@ def test_extendable_generation_alone_is_allowed_under_security():
     a, b = O.solve(plain.problem, params), O.solve(secure.problem, params)
     assert a.status.name == b.status.name == "OPTIMAL"
     assert b.objective_value >= a.objective_value - 1e-6 * abs(a.objective_value)
+
+
+def test_a_state_of_charge_set_point_is_honoured_and_costs_something():
+    """LopfSuite.scala:557-593: pinning one unit's state of charge at every
+    snapshot holds it there, leaves the others free, and costs more."""
+    from oracle import oracle as O
+    free_net = X.network("storage-cycle")
+    free_model = lopf.build(free_net)
+    unconstrained = O.solve(free_model.problem, X.PARAMS).objective_value
+    n = X.network("storage-cycle")
+    units = n.table("StorageUnit")
+    units.static["state_of_charge_set"] = {u: (90.0 if u == "battery" else float("nan")) for u in units.ids}
+    model = lopf.build(n)
+    res = lopf.LopfResult(n, model, O.solve(model.problem, X.PARAMS))
+    assert res.status.name == "OPTIMAL"
+    for t in range(len(n.snapshots)):
+        assert res.state_of_charge("battery", t) == pytest.approx(90.0, abs=1e-4)
+    others = [u for u in units.ids if u != "battery"]
+    assert max(res.state_of_charge(u, t) for u in others for t in range(len(n.snapshots))) > 1.0
+    assert res.objective > unconstrained + 1.0
+
+
+def test_a_storage_power_set_point_is_refused():
+    n = X.network("storage-cycle")
+    units = n.table("StorageUnit")
+    units.static["p_set"] = dict.fromkeys(units.ids, 10.0)
+    with pytest.raises(lopf.UnsupportedNetwork, match="p_set"):
+        lopf.build(n)
+
+
+def test_a_discharge_only_extendable_unit_has_no_nan_bound():
+    """LopfSuite.scala:876-895: p_min_pu = 0 on an extendable unit gives the
+    charging column [0, inf), not an inf x 0 NaN."""
+    n = X.network("storage-hvdc")
+    units = n.table("StorageUnit")
+    units.static["p_min_pu"] = dict.fromkeys(units.ids, 0.0)
+    model = lopf.build(n)
+    for u in units.ids:
+        for t in range(len(n.snapshots)):
+            j = model.columns[("StorageUnit-p_store", u, t)]
+            assert not np.isnan(model.problem.variable_upper[j])
