@@ -6,8 +6,9 @@ import math
 import numpy as np
 import pytest
 
-from noaidi_b200.prima import bnb
+from noaidi_b200.prima import PdhgParams, bnb
 from noaidi_b200.prima.bnb import MilpStatus
+from noaidi_b200.prima.model import LpBuilder
 from tests import bnb_fixtures as X
 
 P = X.PARAMS
@@ -93,3 +94,61 @@ def test_pruning_margin_only_costs_nodes():
     for r in (bare, margined):
         assert r.status == MilpStatus.OPTIMAL and r.objective_value == pytest.approx(optimum, abs=1e-6)
     assert margined.nodes_explored >= bare.nodes_explored
+
+
+def test_an_unconverged_relaxation_downgrades_and_is_counted():
+    """BranchAndBoundSuite.scala:213-223: starved nodes prove nothing, so the
+    result is not conclusive and says how many nodes were unproven."""
+    starved = P.copy(lp=PdhgParams(eps_abs=1e-14, eps_rel=1e-14, max_iterations=2))
+    m = bnb.solve_with(X.knapsackish(), {0, 1}, starved, X.oracle_node_solver(X.knapsackish()))
+    assert m.status != MilpStatus.OPTIMAL and not m.status.is_conclusive
+    assert m.unproven_nodes > 0
+
+
+def test_a_warm_start_from_an_unusable_solution_is_declined():
+    """BranchAndBoundSuite.scala:225-250: a non-finite iterate cannot seed a
+    child; WarmStart refuses it and the search declines rather than throws."""
+    from noaidi_b200.prima.types import KktError, LpSolution, SolveStatus, WarmStart
+    poisoned = LpSolution(SolveStatus.NUMERICAL_ERROR, np.array([1.0, 2.0]), np.array([math.nan]),
+                          np.array([0.0, 0.0]), 1.0, 1.0, 1, 0, 0, KktError(0.0, 0.0, 1.0, 1.0))
+    with pytest.raises(ValueError):
+        WarmStart.from_solution(poisoned)
+    from oracle import oracle as O
+    good = O.solve(X.knapsackish(), P.lp)
+    assert WarmStart.from_solution(good) is not None
+
+
+def test_an_unbounded_relaxation_is_reported_unbounded():
+    b = LpBuilder(1)
+    b.objective_coefficient(0, -1.0)
+    b.bounds(0, 0.0, math.inf)
+    p = b.build()[0]
+    assert run(p, {0}).status == MilpStatus.UNBOUNDED
+
+
+def test_a_time_limit_stops_the_search_without_claiming_optimality():
+    """BranchAndBoundSuite.scala:261-288 on the sixteen-item knapsack."""
+    p = X.hard_knapsack()[0]
+    ints = set(range(p.num_variables))
+    full = run(p, ints)
+    assert full.status == MilpStatus.OPTIMAL and full.nodes_explored > 50
+    limited = run(p, ints, P.copy(time_limit_millis=0))
+    assert limited.nodes_explored <= full.nodes_explored
+    if full.solve_time_millis > 5:
+        assert limited.status != MilpStatus.OPTIMAL and limited.nodes_explored < full.nodes_explored
+
+
+def test_the_reported_objective_is_that_of_the_reported_point():
+    p = X.knapsackish()
+    m = run(p, {0, 1})
+    assert m.status == MilpStatus.OPTIMAL
+    assert m.objective_value == pytest.approx(p.primal_objective(m.primal), abs=1e-12)
+
+
+def test_no_answer_means_no_point_on_the_short_circuit_path():
+    b = LpBuilder(1)
+    b.objective_coefficient(0, 1.0)
+    b.bounds(0, 0.0, 1.0)
+    b.equality_constraint([(0, 1.0)], 5.0)  # outside the box
+    m = run(b.build()[0], set())
+    assert m.status == MilpStatus.INFEASIBLE and m.primal.size == 0
