@@ -228,3 +228,17 @@ class WarmStart:
         return WarmStart(np.array(solution.primal, dtype=np.float64), np.array(solution.dual, dtype=np.float64),
                          s if (math.isfinite(s) and s > 0.0) else None,
                          w if (math.isfinite(w) and w > 0.0) else None)
+
+    def save(self, path: str) -> None:
+        """The four-tuple to disk (numpy .npz), exactly: a solve resumed from
+        ``load(path)`` is the one resumed from this object."""
+        np.savez(path, primal=self.primal, dual=self.dual,
+                 step_size=np.float64(math.nan if self.step_size is None else self.step_size),
+                 primal_weight=np.float64(math.nan if self.primal_weight is None else self.primal_weight))
+
+    @staticmethod
+    def load(path: str) -> "WarmStart":
+        with np.load(path) as f:
+            s, w = float(f["step_size"]), float(f["primal_weight"])
+            return WarmStart(np.array(f["primal"], dtype=np.float64), np.array(f["dual"], dtype=np.float64),
+                             None if math.isnan(s) else s, None if math.isnan(w) else w)
