@@ -20,6 +20,7 @@
 
 #include "prima_internal.h"
 #include "prima_model.h"
+#include "prima_nvtx.h"
 
 namespace prima {
 namespace model {
@@ -561,6 +562,7 @@ class MpsReader {
 
 // Lines end at LF, CR or CR LF, as Source.getLines and linesIterator split them.
 Instance read_text(const char *text, int64_t length, const std::string &fallback) {
+  NvtxRange range("prima: read MPS");
   MpsReader reader(fallback);
   int64_t i = 0;
   while (i < length) {
@@ -608,6 +610,7 @@ void transpose(const Lp &a, std::vector<int32_t> *tp, std::vector<int32_t> *tci,
 }
 
 void presolve(Presolved &P, int32_t max_passes) {
+  NvtxRange range("prima: presolve");
   const Lp &A = P.original;
   const int32_t n = A.n, m = A.m, neq = A.neq;
   transpose(A, &P.tp, &P.tci, &P.tv);

@@ -20,6 +20,7 @@
 #include <cmath>
 
 #include "prima_internal.h"
+#include "prima_nvtx.h"
 
 namespace prima {
 namespace {
@@ -173,6 +174,7 @@ static double device_spectral_bound(const PreparedLp &P, const double *vals, cud
 }
 
 int32_t PreparedLp::prepare(const prima_lp *lp, const prima_params *p, cudaStream_t s) {
+  NvtxRange range("prima: equilibrate and transpose");
   int32_t rc;
   n = lp->num_variables;
   m = lp->num_constraints;

@@ -14,6 +14,7 @@
 #include <math_constants.h>
 
 #include "prima_internal.h"
+#include "prima_nvtx.h"
 #include "prima_solver.cuh"
 
 namespace prima {
@@ -1757,6 +1758,7 @@ struct Job {
 // anchored mode, the tile tables.
 template <typename T>
 int32_t prepare_job(Ctx *c, Job<T> &j) {
+  NvtxRange range("prima: prepare solve");
   int32_t rc;
   if ((rc = check_warm(*j.L, j.req.warm))) return rc;
   PreparedLp &L = *j.L;
@@ -2011,6 +2013,7 @@ int32_t wait_forwarding_cancel(Ctx *c, cudaEvent_t done, const volatile int32_t 
 template <typename T>
 int32_t launch_timed(Ctx *c, const void *kernel, int blocks, void **kargs, const volatile int32_t *cancel,
                      float *kms) {
+  NvtxRange range("prima: persistent PDHG launch");
   cudaStream_t s = c->stream;
   cudaEvent_t e0, e1;
   PRIMA_CUDA_TRY(cudaEventCreate(&e0));
