@@ -1934,7 +1934,7 @@ int32_t setup_job(Ctx *c, Job<T> &j, char *base, const StateLayout<T> &S, int bl
 // After the launch: the final Control record, the solution in caller units
 // and the info fields.  kms: the launch's device time.
 template <typename T>
-int32_t finish_job(Ctx *c, Job<T> &j, float kms, int blocks) {
+int32_t finish_job(Ctx * /*c*/, Job<T> &j, float kms, int blocks) {
   const SolveRequest &req = j.req;
   const dev::Args<T> &a = j.a;
   const int32_t n = j.L->n, m = j.L->m;
