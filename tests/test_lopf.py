@@ -457,3 +457,24 @@ def test_a_discharge_only_extendable_unit_has_no_nan_bound():
         for t in range(len(n.snapshots)):
             j = model.columns[("StorageUnit-p_store", u, t)]
             assert not np.isnan(model.problem.variable_upper[j])
+
+
+def test_the_co2_cap_is_respected_and_reached():
+    """LopfSuite.scala:677-712: emissions, summed with the generators
+    weighting (named here independently of the builder), stay under the cap
+    and reach it -- an absent or mis-signed row exceeds it, an over-tight one
+    stays well below."""
+    from oracle import oracle as O
+    n = X.network("ac-dc-co2")
+    model = lopf.build(n)
+    res = lopf.LopfResult(n, model, O.solve(model.problem, X.PARAMS))
+    gens, carriers = n.table("Generator"), n.table("Carrier")
+    emitted = 0.0
+    for t in range(len(n.snapshots)):
+        for g in gens.ids:
+            intensity = float(carriers.value("co2_emissions", str(gens.value("carrier", g))))
+            emitted += res.dispatch("Generator", g, t) * intensity / gens.at("efficiency", g, t) * \
+                n.weighting("generators", t)
+    cap = float(n.table("GlobalConstraint").value("constant", "co2_limit"))
+    assert emitted <= cap + 1e-6 * max(1.0, cap)
+    assert emitted >= cap - 1e-3 * max(1.0, cap)
