@@ -85,10 +85,11 @@ class Table:
         return attribute in self.static or attribute in self.series
 
     def value(self, attribute: str, entity: str):
-        """A static attribute (PyPSA's default when the file omits it)."""
+        """A static attribute: PyPSA's default where the file omits the column
+        or leaves the cell empty; an explicit NaN stays NaN."""
         if attribute in self.static:
-            v = self.static[attribute][entity]
-            if not (isinstance(v, float) and math.isnan(v)):
+            v = self.static[attribute].get(entity)
+            if v is not None:
                 return v
         return DEFAULTS.get(self.component, {}).get(attribute, math.nan)
 
@@ -122,14 +123,20 @@ LABELS = frozenset({"bus", "bus0", "bus1", "bus2", "bus3", "carrier", "control",
 
 
 def _coerce(v, label: bool = False):
+    """A cell: an empty one is absent (None: the attribute's default
+    applies), the text nan an explicit NaN (CsvReader.scala:150-221)."""
     if v is None or (isinstance(v, float) and math.isnan(v)):
-        return math.nan
+        return None
+    if isinstance(v, str) and v.strip() == "":
+        return None
     if label:
         return str(v)
     if isinstance(v, str):
         t = v.strip()
         if t.lower() in ("true", "false"):
             return t.lower() == "true"
+        if t.lower() in ("nan", "na"):
+            return math.nan
         try:
             return float(t)
         except ValueError:
@@ -142,7 +149,7 @@ def _coerce(v, label: bool = False):
 def read_table(path: str, component: str):
     """One component list file (first column the names) as a Table of
     static attributes, or None when it has no rows."""
-    df = pd.read_csv(path, dtype=str, keep_default_na=True)
+    df = pd.read_csv(path, dtype=str, keep_default_na=False)
     if df.empty:
         return None
     ids = [str(v) for v in df[df.columns[0]]]

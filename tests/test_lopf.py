@@ -478,3 +478,71 @@ def test_the_co2_cap_is_respected_and_reached():
     cap = float(n.table("GlobalConstraint").value("constant", "co2_limit"))
     assert emitted <= cap + 1e-6 * max(1.0, cap)
     assert emitted >= cap - 1e-3 * max(1.0, cap)
+
+
+def test_a_nan_capacity_floor_is_refused():
+    """LopfSuite.scala:434-450: a NaN p_nom_min is not a capacity."""
+    n = X.network("ac-dc-meshed")
+    gens = n.table("Generator")
+    g = next(i for i in gens.ids if lopf.extendable(gens, i))
+    gens.static.setdefault("p_nom_min", {})[g] = float("nan")
+    with pytest.raises(lopf.UnsupportedNetwork, match="p_nom_min"):
+        lopf.build(n)
+
+
+def _series(tab, attr, values_by_id, T):
+    arr = np.array([[values_by_id.get(i, float(tab.value(attr, i))) for i in tab.ids] for _ in range(T)])
+    tab.series[attr] = arr
+
+
+def test_standing_losses_are_checked_where_the_balance_reads_them():
+    """LopfSuite.scala:917-1040: a bad loss given only per snapshot is
+    refused; a bad static loss that a series fully overrides is not; a
+    series on one unit does not excuse a bad static value on another."""
+    T = len(X.network("storage-cycle").snapshots)
+    n = X.network("storage-cycle")
+    _series(n.table("StorageUnit"), "standing_loss", {"battery": 1.5}, T)
+    with pytest.raises(lopf.UnsupportedNetwork, match="standing_loss"):
+        lopf.build(n)
+    n = X.network("storage-cycle")
+    units = n.table("StorageUnit")
+    units.static["standing_loss"] = {u: (1.5 if u == "battery" else 0.0) for u in units.ids}
+    _series(units, "standing_loss", {"battery": 0.01}, T)
+    lopf.build(n)  # the series is what the balance reads
+    n = X.network("storage-cycle")
+    units = n.table("StorageUnit")
+    other = next(u for u in units.ids if u != "battery")
+    units.static["standing_loss"] = {u: (1.5 if u == other else 0.0) for u in units.ids}
+    units.series["standing_loss"] = np.array([[0.01 if u == "battery" else 1.5 for u in units.ids]
+                                              for _ in range(T)])
+    with pytest.raises(lopf.UnsupportedNetwork, match=other):
+        lopf.build(n)
+
+
+def test_an_extendable_stores_energy_is_free_at_both_ends():
+    """LopfSuite.scala:934-967: e_min_pu may be negative, so an extendable
+    store's energy column carries both ends in rows, not a zero bound."""
+    n = X.network("store-bank")
+    model = lopf.build(n)
+    st = n.table("Store")
+    ext = [i for i in st.ids if lopf.extendable(st, i)]
+    assert ext
+    for s_ in ext:
+        for t in range(len(n.snapshots)):
+            j = model.columns[("Store-e", s_, t)]
+            assert model.problem.variable_lower[j] == -np.inf and model.problem.variable_upper[j] == np.inf
+
+
+def test_the_storage_fixtures_flags_are_load_bearing():
+    """LopfSuite.scala:488-517: PyPSA's storage-cycle answer uses every
+    feature the fixture sets -- a cyclic unit ends holding energy, a unit
+    spills, and the standing loss is non-zero where set."""
+    exp = X.expected("storage-cycle")
+    n = X.network("storage-cycle")
+    units = n.table("StorageUnit")
+    T = len(n.snapshots)
+    spilled = sum(X.frame_value(exp["storage_spill"], t, u) for t in range(T) for u in units.ids)
+    assert spilled > 1.0
+    cyclic = [u for u in units.ids if bool(units.value("cyclic_state_of_charge", u)) is True]
+    assert cyclic and max(X.frame_value(exp["storage_state_of_charge"], T - 1, u) for u in cyclic) > 1.0
+    assert any(float(units.value("standing_loss", u)) > 0.0 for u in units.ids)
