@@ -546,3 +546,72 @@ def test_the_storage_fixtures_flags_are_load_bearing():
     cyclic = [u for u in units.ids if bool(units.value("cyclic_state_of_charge", u)) is True]
     assert cyclic and max(X.frame_value(exp["storage_state_of_charge"], T - 1, u) for u in cyclic) > 1.0
     assert any(float(units.value("standing_loss", u)) > 0.0 for u in units.ids)
+
+
+def _cycles_network(tmp_path, buses, lines, carrier="AC", v_nom=1.0, x=1.0, r=0.0):
+    from noaidi_b200.network.pypsa_csv import read
+    d = tmp_path / "net"
+    d.mkdir(exist_ok=True)
+    (d / "buses.csv").write_text("name,v_nom,carrier\n" + "".join(f"{b},{v_nom},{carrier}\n" for b in buses))
+    (d / "lines.csv").write_text("name,bus0,bus1,x,r,s_nom\n" +
+                                 "".join(f"{i},{a},{b},{x},{r},100.0\n" for i, a, b in lines))
+    (d / "snapshots.csv").write_text(",snapshot\n0,2015-01-01 00:00:00\n")
+    return read(str(d), "cycles")
+
+
+def _signs(cycle):
+    return {e: o for _, e, o in cycle.terms}
+
+
+def test_a_triangle_gives_one_consistently_traversed_cycle(tmp_path):
+    """CyclesSuite.scala:54-71: head-to-tail lines, one cycle, one sign."""
+    cycles = lopf.cycle_basis(_cycles_network(tmp_path, "LMN", [("a", "L", "M"), ("b", "M", "N"), ("c", "N", "L")]))
+    assert len(cycles) == 1
+    s = _signs(cycles[0])
+    assert set(s) == {"a", "b", "c"} and len(set(s.values())) == 1 and abs(s["a"]) == 1.0
+
+
+def test_a_parallel_pair_gives_opposing_branches(tmp_path):
+    cycles = lopf.cycle_basis(_cycles_network(tmp_path, "AB", [("a", "A", "B"), ("b", "A", "B")]))
+    assert len(cycles) == 1
+    s = _signs(cycles[0])
+    assert set(s) == {"a", "b"} and s["a"] == -s["b"]
+
+
+def test_a_tree_has_no_cycles(tmp_path):
+    assert lopf.cycle_basis(_cycles_network(tmp_path, "ABCD", [("a", "A", "B"), ("b", "B", "C"), ("c", "B", "D")])) == []
+
+
+def test_two_independent_loops_give_one_cycle_per_component(tmp_path):
+    lines = [("a", "A", "B"), ("b", "B", "C"), ("c", "C", "A"), ("x", "X", "Y"), ("y", "Y", "Z"), ("z", "Z", "X")]
+    cycles = lopf.cycle_basis(_cycles_network(tmp_path, "ABCXYZ", lines))
+    assert len(cycles) == 2
+    assert {e for c in cycles for e in _signs(c)} == {"a", "b", "c", "x", "y", "z"}
+
+
+def test_a_square_with_a_chord_gives_two_closed_triangles(tmp_path):
+    """CyclesSuite.scala:110-128: each basis cycle is a triangle and a closed
+    walk -- every bus it touches entered and left once."""
+    lines = [("a", "A", "B"), ("b", "B", "C"), ("c", "C", "D"), ("d", "D", "A"), ("e", "A", "C")]
+    ends = {i: (p, q) for i, p, q in lines}
+    cycles = lopf.cycle_basis(_cycles_network(tmp_path, "ABCD", lines))
+    assert len(cycles) == 2
+    for c in cycles:
+        s = _signs(c)
+        assert len(s) == 3 and all(abs(o) == 1.0 for o in s.values())
+        net = {}
+        for e, o in s.items():  # o x (out of bus0, into bus1) must cancel at every bus
+            p, q = ends[e]
+            net[p] = net.get(p, 0.0) - o
+            net[q] = net.get(q, 0.0) + o
+        assert all(v == 0.0 for v in net.values()), net
+
+
+def test_cycles_over_a_dc_island_use_resistance(tmp_path):
+    """CyclesSuite.scala:130-: with x = 0 and r = 0.5 over v_nom 2, the
+    Kirchhoff coefficients are +-0.5 / 4, not zero."""
+    n = _cycles_network(tmp_path, "ABC", [("a", "A", "B"), ("b", "B", "C"), ("c", "C", "A")], carrier="DC",
+                        v_nom=2.0, x=0.0, r=0.5)
+    [cycle] = lopf.cycle_basis(n)
+    for _, e, _ in cycle.terms:
+        assert lopf.impedance(n, "Line", e, cycle.carrier) == pytest.approx(0.5 / 4.0)
