@@ -615,3 +615,54 @@ def test_cycles_over_a_dc_island_use_resistance(tmp_path):
     [cycle] = lopf.cycle_basis(n)
     for _, e, _ in cycle.terms:
         assert lopf.impedance(n, "Line", e, cycle.carrier) == pytest.approx(0.5 / 4.0)
+
+
+def _triangle_with_spur():
+    n = X.network("sclopf-triangle")
+    lines = n.table("Line")
+    lines.ids.append("CD")
+    for attr, v in (("bus0", "C"), ("bus1", "D"), ("x", 0.1), ("s_nom", 150.0)):
+        lines.static.setdefault(attr, {})["CD"] = v
+    n.table("Bus").ids.append("D")
+    n.table("Bus").static.setdefault("v_nom", {})["D"] = 380.0
+    return n
+
+
+def test_an_unrequested_bridge_column_is_marked_not_computed():
+    """SclopfSuite.scala:368-393: with only AB requested, AB's and BC's
+    columns are computed and the bridge CD's is not -- marked so rather than
+    read as a zero meaning no effect."""
+    n = _triangle_with_spur()
+    [(carrier, buses, branches)] = lopf.sub_networks(n)
+    names, factors, populated = lopf.lodf(n, carrier, buses, branches, {("Line", "AB")})
+    at = {key: k for k, key in enumerate(names)}
+    assert populated[at[("Line", "AB")]] and abs(factors[at[("Line", "BC")], at[("Line", "AB")]]) > 0.0
+    assert populated[at[("Line", "BC")]] and abs(factors[at[("Line", "AB")], at[("Line", "BC")]]) > 0.0
+    assert not populated[at[("Line", "CD")]]
+
+
+@pytest.mark.parametrize("ratio", [1e2, 1e4, 1e6])
+def test_factors_stay_bounded_near_a_bridge(tmp_path, ratio):
+    """SclopfSuite.scala:395-424: a stiff branch beside a path ratio times
+    weaker -- losing either moves all its flow, so every factor is at most
+    one in magnitude, however close the network is to a bridge."""
+    n = _cycles_network(tmp_path, "ABC", [("AB", "A", "B"), ("AC", "A", "C"), ("CB", "C", "B")], v_nom=380.0)
+    lines = n.table("Line")
+    lines.static["x"] = {"AB": 0.1, "AC": 0.1 * ratio, "CB": 0.1 * ratio}
+    [(carrier, buses, branches)] = lopf.sub_networks(n)
+    _, factors, populated = lopf.lodf(n, carrier, buses, branches)
+    off = [abs(factors[i, j]) for i in range(3) for j in range(3) if i != j and populated[j]]
+    assert max(off) == pytest.approx(1.0, abs=1e-6)
+
+
+def test_an_extendable_transformer_is_refused_under_security():
+    n = X.network("transformer-levels")
+    tr = n.table("Transformer")
+    tr.static["s_nom_extendable"] = dict.fromkeys(tr.ids, True)
+    with pytest.raises(lopf.UnsupportedNetwork, match="Transformer"):
+        lopf.build_sclopf(n, [("Line", "hv")])
+
+
+def test_an_empty_outage_list_is_the_dispatch_model_even_when_extendable():
+    n = X.network("ac-dc-meshed")
+    assert lopf.build_sclopf(n, []).problem.num_constraints == lopf.build(n).problem.num_constraints
