@@ -383,6 +383,29 @@ def impedance(network: Network, component: str, entity: str, carrier: str) -> fl
     raise UnsupportedNetwork(f"{component} '{entity}' is a passive branch whose per-unit base is not known here")
 
 
+def susceptance(network: Network, component: str, entity: str, carrier: str) -> float:
+    """Per-unit susceptance of a branch in the outage factors
+    (``Branches.susceptance``, modules/network-pf/.../Branches.scala:67-106):
+    the reciprocal of the Kirchhoff-row impedance, but strict where that one
+    is lenient -- a reactance (resistance in DC) that is not positive, or a
+    line whose bus0 has no positive v_nom, has no susceptance and is
+    refused."""
+    tab = network.table(component)
+    name = "r" if carrier == "DC" else "x"
+    z = float(tab.value(name, entity))
+    if not z > 0.0:
+        raise UnsupportedNetwork(f"{component} '{entity}' has {name} = {z} in a {carrier} sub-network, so it has "
+                                 "no susceptance")
+    if component == "Line":
+        bus0 = str(tab.value("bus0", entity))
+        v = float(network.table("Bus").value("v_nom", bus0))
+        if not v > 0.0:
+            raise UnsupportedNetwork(f"bus '{bus0}' has v_nom = {v}, so Line '{entity}' has no per-unit base; "
+                                     "every branch in a sub-network must share one")
+        return v * v / z
+    return 1.0 / impedance(network, component, entity, carrier)
+
+
 def build(network: Network) -> Model:
     network = standard_types.expand(network)  # impedance named by type (Lopf.scala:73)
     _reject(network)
@@ -646,9 +669,10 @@ def lodf(network: Network, carrier: str, buses: list, branches: list, outages: O
     modules/network-pf/.../Lodf.scala): PTDF = diag(b) A B^-1 with the first
     bus as reference (the factors do not depend on that choice), and
     LODF[l, o] = PTDF_l(o) / (1 - PTDF_o(o)), -1 on the diagonal, with b the
-    per-unit susceptance of the Kirchhoff rows.  A bridge (a denominator
-    within 1e-7 of zero) has no post-outage flow: it is refused if requested
-    as a contingency and left unpopulated otherwise.  ``branches`` are
+    per-unit ``susceptance``.  A bridge (a denominator within 1e-7 of zero)
+    has no post-outage flow: it is refused if requested as a contingency and
+    left unpopulated otherwise; a requested column with a non-finite factor
+    is refused too (Lodf.scala:187-230).  ``branches`` are
     (component, id) keys.  Returns (branches, factors m x m, populated per
     outage column)."""
     m = len(branches)
@@ -656,7 +680,7 @@ def lodf(network: Network, carrier: str, buses: list, branches: list, outages: O
         return [], np.zeros((0, 0)), np.zeros(0, dtype=bool)
     index = {b: i for i, b in enumerate(buses[1:])}
     n = len(index)
-    y = np.array([1.0 / impedance(network, c, i, carrier) for c, i in branches])
+    y = np.array([susceptance(network, c, i, carrier) for c, i in branches])
     A = np.zeros((m, n))
     for k, (c, i) in enumerate(branches):
         tab = network.table(c)
@@ -685,6 +709,9 @@ def lodf(network: Network, carrier: str, buses: list, branches: list, outages: O
         populated[j] = True
         factors[:, j] = branch_ptdf[:, j] / denominator
         factors[j, j] = -1.0
+        if requested and not np.isfinite(factors[:, j]).all():
+            raise UnsupportedNetwork(f"outage of {key[0]} '{key[1]}' gives a non-finite factor, so its "
+                                     "sub-network's susceptance matrix did not solve cleanly")
     return branches, factors, populated
 
 

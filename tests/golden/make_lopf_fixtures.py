@@ -1,7 +1,8 @@
 """Copies PyPSA's standard type library into noaidi_b200/network/
 standard_types/, and the input tables of PyPSA golden networks and the expected LOPF
 results (objective, generator dispatch, line flows, storage trajectories,
-optimal capacities and the objective constant) from the reference's
+optimal capacities, the objective constant and PyPSA's branch outage
+distribution factors) from the reference's
 goldens (reference/goldens/{networks,results} in oluies/noaidi, generated by
 PyPSA 1.2.4) into tests/golden/lopf/<network>/.
 
@@ -79,6 +80,8 @@ def main(root):
         if "sclopf" in full:  # the security-constrained solve, with the outages PyPSA used
             keep["sclopf"] = {k: full["sclopf"][k] for k in ("branch_outages", "objective", "status", "generator_p",
                                                              "line_p0")}
+        if isinstance(full.get("bodf"), dict) and "error" not in full["bodf"]:  # PyPSA's BODF per sub-network
+            keep["bodf"] = full["bodf"]
         with open(os.path.join(dst, "expected.json"), "w") as f:
             json.dump(keep, f, indent=1)
         print(name, "->", dst)

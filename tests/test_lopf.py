@@ -666,3 +666,92 @@ def test_an_extendable_transformer_is_refused_under_security():
 def test_an_empty_outage_list_is_the_dispatch_model_even_when_extendable():
     n = X.network("ac-dc-meshed")
     assert lopf.build_sclopf(n, []).problem.num_constraints == lopf.build(n).problem.num_constraints
+
+
+BODF_NETWORKS = [n for n in X.NETWORKS if "bodf" in X.expected(n)]
+
+
+def _our_factors(n):
+    """Every populated (affected, outage) factor over all sub-networks, with
+    no contingency requested so that a bridge is left unpopulated."""
+    from noaidi_b200.network import standard_types
+    n = standard_types.expand(n)
+    out, bridges = {}, set()
+    for carrier, buses, branches in lopf.sub_networks(n):
+        keys, f, populated = lopf.lodf(n, carrier, buses, branches, set())
+        for j, o in enumerate(keys):
+            if not populated[j]:
+                bridges.add(o)
+                continue
+            for i, a in enumerate(keys):
+                out[(a, o)] = f[i, j]
+    return out, bridges
+
+
+@pytest.mark.parametrize("name", BODF_NETWORKS)
+def test_outage_factors_match_pypsa_bodf(name):
+    """LodfSuite.scala:32-65, over every golden network PyPSA computed a
+    BODF for: the same branches per sub-network and every factor within
+    1e-9; the only columns left out are bridges, whose PyPSA column is the
+    -1 diagonal of a one-branch island."""
+    ours, bridges = _our_factors(X.network(name))
+    ours_branches = {a for a, _ in ours} | bridges
+    compared = 0
+    for block in X.expected(name)["bodf"].values():
+        keys = [tuple(b) for b in block["branches"]]
+        assert set(keys) <= ours_branches
+        for i, a in enumerate(keys):
+            for j, o in enumerate(keys):
+                if o in bridges:
+                    assert len(keys) == 1 and block["bodf"][i][j] == pytest.approx(-1.0)
+                    continue
+                assert ours[(a, o)] == pytest.approx(block["bodf"][i][j], abs=1e-9), (a, o)
+                compared += 1
+    assert compared == len(ours)
+
+
+def test_the_meshed_fixture_can_tell_a_stub_from_the_factors():
+    """LodfSuite.scala:54-64: at least six off-diagonal factors of lodf-mesh
+    differ from +-1, which a stub returning +-1 would get wrong."""
+    block = next(iter(X.expected("lodf-mesh")["bodf"].values()))
+    m = len(block["branches"])
+    assert sum(1 for i in range(m) for j in range(m)
+               if i != j and abs(abs(block["bodf"][i][j]) - 1.0) > 1e-6) >= 6
+
+
+def test_a_single_cycle_gives_factors_of_magnitude_one():
+    """LodfSuite.scala:67-79: one cycle has one alternative path, so every
+    factor is +-1 whatever the impedances."""
+    ours, _ = _our_factors(X.network("sclopf-triangle"))
+    for a, o in (("AB", "BC"), ("AB", "AC"), ("BC", "AC")):
+        assert abs(ours[(("Line", a), ("Line", o))]) == pytest.approx(1.0, abs=1e-9)
+
+
+@pytest.mark.parametrize("x", [0.0, -0.1, float("nan")])
+def test_a_branch_without_susceptance_is_refused_by_the_outage_factors(x):
+    """Branches.susceptance (Branches.scala:74-79): the factors refuse a
+    reactance that is not positive, where the Kirchhoff rows would carry it."""
+    n = X.network("lodf-mesh")
+    n.table("Line").static["x"]["AB"] = x
+    [(carrier, buses, branches)] = lopf.sub_networks(n)
+    with pytest.raises(lopf.UnsupportedNetwork, match="no susceptance"):
+        lopf.lodf(n, carrier, buses, branches, set())
+
+
+def test_a_line_at_a_bus_without_voltage_is_refused_by_the_outage_factors():
+    n = X.network("lodf-mesh")
+    bus0 = str(n.table("Line").value("bus0", "AB"))
+    n.table("Bus").static.setdefault("v_nom", {})[bus0] = 0.0
+    [(carrier, buses, branches)] = lopf.sub_networks(n)
+    with pytest.raises(lopf.UnsupportedNetwork, match="v_nom"):
+        lopf.lodf(n, carrier, buses, branches, set())
+
+
+def test_a_non_finite_factor_is_refused_for_a_requested_outage():
+    """Lodf.scala:224-229: a reactance so small its susceptance overflows
+    gives non-finite factors; a requested contingency refuses them."""
+    n = X.network("lodf-mesh")
+    n.table("Line").static["x"]["AB"] = 1e-310
+    [(carrier, buses, branches)] = lopf.sub_networks(n)
+    with np.errstate(all="ignore"), pytest.raises(lopf.UnsupportedNetwork, match="non-finite"):
+        lopf.lodf(n, carrier, buses, branches, {("Line", "AB")})
