@@ -64,7 +64,7 @@ import numpy as np
 from ..prima.model import LpBuilder, LpProblem, Negated, RowTranslation
 from ..prima.types import LpSolution, PdhgParams, SolveStatus
 from . import standard_types
-from .pypsa_csv import Network
+from .pypsa_csv import LIST_NAMES, MalformedNetwork, Network
 
 HANDLED = {"Bus", "Carrier", "Generator", "Load", "Line", "Transformer", "Link", "GlobalConstraint", "SubNetwork",
            "LineType", "TransformerType", "Shape", "StorageUnit", "Store"}
@@ -215,26 +215,56 @@ def _reject(network: Network) -> None:
             ("marginal_cost_quadratic" in st.series and np.any(st.series["marginal_cost_quadratic"] != 0.0)):
         raise UnsupportedNetwork("a Store has a non-zero marginal_cost_quadratic; the objective here is linear")
     _reject_standing_loss(network, st)
-    buses = set(network.table("Bus").ids)
-    links = network.table("Link")
-    if len(links):
-        for required in ("bus0", "bus1"):  # Topology.portsOf: a branch needs both endpoints
-            if required not in links.static:
-                raise UnsupportedNetwork(f"links has no '{required}' column; a branch needs both endpoints")
-    for comp, ports in (("Generator", ("bus",)), ("Load", ("bus",)), ("StorageUnit", ("bus",)), ("Store", ("bus",)),
-                        ("Line", ("bus0", "bus1")), ("Transformer", ("bus0", "bus1")),
-                        ("Link", tuple(link_ports(links)))):
+    dangling = dangling_bus_references(network)  # Lopf.rejectDanglingBuses (Lopf.scala:593-606)
+    if dangling:
+        comp, i, port, bus = dangling[0]
+        raise UnsupportedNetwork(f"{comp} '{i}' references unknown bus '{bus}' via {port}")
+
+
+BRANCHES = PASSIVE + ("Link",)
+ONE_PORTS = ("Generator", "Load", "StorageUnit", "Store")
+
+
+def _ports(network: Network, component: str) -> list:
+    """``Topology.portsOf`` (Topology.scala:212-232): a branch table's bus
+    columns in port order; one without bus0 or bus1 is malformed."""
+    tab = network.table(component)
+    if not len(tab):
+        return []
+    for required in ("bus0", "bus1"):
+        if required not in tab.static:
+            raise MalformedNetwork(f"{LIST_NAMES[component]} has no '{required}' column; a branch needs both "
+                                   "endpoints")
+    return link_ports(tab) if component == "Link" else ["bus0", "bus1"]
+
+
+def dangling_references(network: Network, components=BRANCHES) -> list:
+    """``Topology.danglingReferences`` (Topology.scala:277-326): every
+    (component, id, port, bus) of a branch naming no bus.  A blank bus0 or
+    bus1 is dangling; a blank further port (a two-port link in a table with
+    a bus2 column) is not connected, and not an error."""
+    known = set(network.table("Bus").ids)
+    out = []
+    for comp in components:
         tab = network.table(comp)
-        for i in tab.ids:
-            for port in ports:
-                if port not in ("bus", "bus0", "bus1") and not _named(tab.value(port, i)):
-                    continue  # a later port a link leaves empty: not connected
-                if str(tab.value(port, i)) not in buses:
-                    raise UnsupportedNetwork(f"{comp} '{i}' references unknown bus '{tab.value(port, i)}' via {port}")
+        for port in _ports(network, comp):
+            for i in tab.ids:
+                bus = tab.endpoint(port, i)
+                if (bus not in known) if bus else port in ("bus0", "bus1"):
+                    out.append((comp, i, port, bus))
+    return out
 
 
-def _named(v) -> bool:
-    return isinstance(v, str) and v.strip() != ""
+def dangling_bus_references(network: Network) -> list:
+    """``Topology.danglingBusReferences`` (Topology.scala:293-307): the
+    branches' dangling references, then every one-port component whose bus
+    names no bus (a stale load would simply vanish from the balance)."""
+    known = set(network.table("Bus").ids)
+    out = dangling_references(network)
+    for comp in ONE_PORTS:
+        tab = network.table(comp)
+        out += [(comp, i, "bus", tab.endpoint("bus", i)) for i in tab.ids if tab.endpoint("bus", i) not in known]
+    return out
 
 
 def link_ports(links) -> list:
@@ -307,11 +337,14 @@ def cycle_basis(network: Network) -> list:
         adjacency.setdefault(e[2], []).append(e)
         adjacency.setdefault(e[3], []).append(e)
     bus_tab = network.table("Bus")
+    # the island's label, read off its first sorted bus rather than this walk's
+    # root, so that a mixed-carrier island picks x or r as Cycles.scala:43-53 does
+    carrier_of = {b: sub.carrier for sub in sub_networks(network) for b in sub.buses}
     visited, cycles = set(), []
     for root in bus_tab.ids:
         if root in visited or root not in adjacency:
             continue
-        carrier = str(bus_tab.value("carrier", root))
+        carrier = carrier_of[root]
         parent, depth = {}, {root: 0}
         tree = set()
         visited.add(root)
@@ -495,14 +528,14 @@ def build(network: Network) -> Model:
         attached[str(stores.value("bus", s_))]["store"].append(s_)
     for d in loads.ids:
         attached[str(loads.value("bus", d))]["load"].append(d)
-    for comp in PASSIVE + ("Link",):
+    for comp in BRANCHES:
         tab = network.table(comp)
-        ports = link_ports(tab) if comp == "Link" else ["bus0", "bus1"]
+        ports = _ports(network, comp)
         for e in tab.ids:  # bus0 first, so a branch looping onto one bus lists -1 then its efficiency
             for port in ports:
-                bus = tab.value(port, e)
-                if _named(bus) and str(bus) in attached:
-                    attached[str(bus)]["branch"].append((comp, e, port))
+                bus = tab.endpoint(port, e)  # '' for a port this link leaves unconnected
+                if bus in attached:
+                    attached[bus]["branch"].append((comp, e, port))
 
     balance_rows, row = {}, 0
     for t in range(T):
@@ -635,32 +668,66 @@ def solve(network: Network, params: PdhgParams = PdhgParams(), precision: int = 
 
 # ---- security-constrained LOPF (N-1) ------------------------------------------
 
+class SubNetwork(tuple):
+    """One island of ``sub_networks``; unpacks as (carrier, buses,
+    branches) and carries ``mixed_carriers`` (``SubNetwork``,
+    Topology.scala:64-75)."""
+
+    def __new__(cls, carrier: str, buses: list, branches: list, mixed_carriers: bool = False):
+        self = super().__new__(cls, (carrier, buses, branches))
+        self.mixed_carriers = mixed_carriers
+        return self
+
+    carrier = property(lambda self: self[0])
+    buses = property(lambda self: self[1])
+    branches = property(lambda self: self[2])  # (component, id) of its passive branches, lines first
+
+
 def sub_networks(network: Network) -> list:
-    """Connected components of the buses over the passive branches, each
-    (carrier, [buses], [(component, id) of its branches]) --
-    ``Topology.subNetworks``."""
-    branches = passive_branches(network)
+    """``Topology.subNetworks`` (modules/network-model/.../Topology.scala:
+    104-161): the buses connected over passive branches -- links join no
+    islands -- with each island's buses sorted, its carrier label that of the
+    first sorted bus, and the islands in order of their first bus.  An island
+    whose buses disagree about carrier keeps that label and is flagged
+    ``mixed_carriers``, as PyPSA warns rather than fails.  A passive branch
+    table without a bus0 or bus1 column, or an endpoint that is blank or
+    names no bus, raises ``MalformedNetwork``: a dropped edge would split an
+    island and still look like a network."""
     bus_tab = network.table("Bus")
-    adjacency: dict = {b: [] for b in bus_tab.ids}
-    for c, i, b0, b1 in branches:
-        adjacency[b0].append(((c, i), b1))
-        adjacency[b1].append(((c, i), b0))
-    seen, out = set(), []
-    for root in bus_tab.ids:
-        if root in seen:
-            continue
-        comp, stack, keys = [], [root], set()
-        seen.add(root)
-        while stack:
-            b = stack.pop()
-            comp.append(b)
-            for key, nb in adjacency[b]:
-                keys.add(key)
-                if nb not in seen:
-                    seen.add(nb)
-                    stack.append(nb)
-        out.append((str(bus_tab.value("carrier", root)), comp,
-                    [(c, i) for c, i, _, _ in branches if (c, i) in keys]))
+    if not bus_tab.ids:
+        return []
+    dangling = dangling_references(network, PASSIVE)
+    if dangling:
+        comp, i, port, bus = dangling[0]
+        more = f" (and {len(dangling) - 1} other dangling reference(s))" if len(dangling) > 1 else ""
+        raise MalformedNetwork(f"{comp} '{i}' references unknown bus '{bus}' via {port}{more}")
+    parent = {b: b for b in bus_tab.ids}
+
+    def find(x):
+        root = x
+        while parent[root] != root:
+            root = parent[root]
+        while parent[x] != root:  # path compression: a long radial feeder stays linear
+            parent[x], x = root, parent[x]
+        return root
+
+    branches = passive_branches(network)
+    for _, _, b0, b1 in branches:
+        r0, r1 = find(b0), find(b1)
+        if r0 != r1:
+            parent[r0] = r1
+    islands: dict = {}
+    for b in bus_tab.ids:
+        islands.setdefault(find(b), []).append(b)
+    out = []
+    for members in islands.values():
+        buses = sorted(members)
+        carriers = list(dict.fromkeys(str(bus_tab.value("carrier", b)) for b in buses))
+        out.append(SubNetwork(carriers[0], buses, [], len(carriers) > 1))
+    out.sort(key=lambda sub: sub.buses[0])
+    island_of = {b: sub for sub in out for b in sub.buses}
+    for c, i, b0, _ in branches:
+        island_of[b0].branches.append((c, i))
     return out
 
 

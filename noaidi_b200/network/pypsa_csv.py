@@ -61,6 +61,12 @@ DEFAULTS = {
 }
 
 
+class MalformedNetwork(ValueError):
+    """``CsvReader.MalformedNetwork``: the files do not describe a network --
+    a branch table without an endpoint column, an endpoint left blank or
+    naming no bus."""
+
+
 @dataclass
 class Table:
     """One component's entities: static attributes and per-snapshot series."""
@@ -83,6 +89,12 @@ class Table:
 
     def has(self, attribute: str) -> bool:
         return attribute in self.static or attribute in self.series
+
+    def endpoint(self, port: str, entity: str) -> str:
+        """A bus reference as written: '' for an empty cell or an absent
+        column (a port has no default, so a blank never names a bus)."""
+        v = self.static.get(port, {}).get(entity)
+        return "" if v is None else str(v)
 
     def value(self, attribute: str, entity: str):
         """A static attribute: PyPSA's default where the file omits the column

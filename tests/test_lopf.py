@@ -227,14 +227,15 @@ def test_scigrid_de_matches_pypsa_at_the_reference_tolerance():
 
 def test_sclopf_expands_types_before_computing_outage_factors():
     """LopfSuite.scala:846-875: on standard-types the contingency rows need
-    the typed impedances; a secure dispatch costs at least the plain one."""
+    the typed impedances; a secure dispatch costs at least the plain one, up
+    to the 1e-9 relative KKT tolerance both solves stop at."""
     from oracle import oracle as O
     n = X.network("standard-types")
     outages = [("Line", "hv12"), ("Line", "hv23"), ("Line", "hv31")]
     model, plain = lopf.build_sclopf(n, outages), lopf.build(n)
     assert model.problem.num_constraints > plain.problem.num_constraints
     a, b = O.solve(plain.problem, X.PARAMS), O.solve(model.problem, X.PARAMS)
-    assert b.status.name == "OPTIMAL" and b.objective_value >= a.objective_value - 1e-6
+    assert b.status.name == "OPTIMAL" and b.objective_value >= a.objective_value * (1 - 1e-8)
 
 
 def _chp_network(efficiency2):
