@@ -1,64 +1,128 @@
-"""A PyPSA CSV network folder read into plain tables: the subset of the
-reference's network model (modules/network-model/.../CsvReader.scala,
-ComponentTable.scala) that the dispatch LOPF needs.
+"""A PyPSA CSV network folder read into plain tables: the reference's
+network model (modules/network-model/.../CsvReader.scala, Schema.scala,
+ComponentTable.scala) as far as the LOPF builders read it.
 
 A folder holds ``<list>.csv`` per component (one row per entity, the first
 column its name), ``<list>-<attribute>.csv`` for attributes that vary by
-snapshot (one row per snapshot, one column per entity), and
-``snapshots.csv`` with the weightings.  Attributes a file leaves out take
-PyPSA's defaults (the schema's ``default`` entries for the attributes used
-here); a varying attribute without a series file takes its static value.
+snapshot (one row per snapshot, one column per entity that varies), and
+``snapshots.csv`` with the weightings.  Every cell is typed by PyPSA's
+component schema (``pypsa_schema.json``, generated from PyPSA 1.2.4's
+registry): a float attribute's cell is a number or refused, a boolean's is
+true only as ``true``, ``1`` or ``1.0``, an integer's is truncated, text is
+trimmed, and a blank cell -- like an omitted column -- takes the schema
+default.  A column the schema does not know is a custom attribute, typed
+from its values.  A varying attribute without a series file, or an entity
+its file does not cover, takes its static value.
 """
 from __future__ import annotations
 
+import json
 import math
 import os
 import re
 from dataclasses import dataclass, field
 
 import numpy as np
-import pandas as pd
 
-# file stem of each component's tables (PyPSA's list names)
-LIST_NAMES = {
-    "Bus": "buses", "Carrier": "carriers", "Generator": "generators", "Load": "loads", "Line": "lines",
-    "Link": "links", "Transformer": "transformers", "StorageUnit": "storage_units", "Store": "stores",
-    "GlobalConstraint": "global_constraints", "SubNetwork": "sub_networks", "ShuntImpedance": "shunt_impedances",
-    "LineType": "line_types", "TransformerType": "transformer_types", "Shape": "shapes", "Process": "processes",
-}
+SCHEMA_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pypsa_schema.json")
+RESERVED = frozenset({"snapshots.csv", "network.csv", "investment_periods.csv"})  # not component tables
 
-# PyPSA's defaults for the attributes the dispatch LOPF reads
-DEFAULTS = {
-    "Bus": {"v_nom": 1.0, "carrier": "AC"},
-    "Generator": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
-                  "p_nom_extendable": False, "committable": False, "carrier": "", "p_nom_min": 0.0,
-                  "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0, "start_up_cost": 0.0,
-                  "shut_down_cost": 0.0, "min_up_time": 0.0, "min_down_time": 0.0, "up_time_before": 1.0,
-                  "down_time_before": 0.0, "stand_by_cost": 0.0, "marginal_cost_quadratic": 0.0,
-                  "ramp_limit_up": math.nan, "ramp_limit_down": math.nan, "ramp_limit_start_up": math.nan,
-                  "ramp_limit_shut_down": math.nan},
-    "Load": {"p_set": 0.0},
-    "Line": {"x": 0.0, "r": 0.0, "b": 0.0, "g": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "s_nom_extendable": False,
-             "s_nom_min": 0.0, "s_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0, "length": 0.0,
-             "num_parallel": 1.0},
-    "Transformer": {"x": 0.0, "r": 0.0, "b": 0.0, "g": 0.0, "s_nom": 0.0, "s_max_pu": 1.0, "tap_ratio": 1.0,
-                    "phase_shift": 0.0, "num_parallel": 1.0, "tap_position": 0.0, "tap_side": 0.0,
-                    "s_nom_extendable": False, "s_nom_min": 0.0, "s_nom_max": math.inf, "capital_cost": 0.0,
-                    "fom_cost": 0.0},
-    "Link": {"p_nom": 0.0, "p_min_pu": 0.0, "p_max_pu": 1.0, "efficiency": 1.0, "marginal_cost": 0.0,
-             "p_nom_extendable": False, "p_nom_min": 0.0, "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
-    "StorageUnit": {"p_nom": 0.0, "p_min_pu": -1.0, "p_max_pu": 1.0, "max_hours": 1.0, "efficiency_store": 1.0,
-                    "efficiency_dispatch": 1.0, "standing_loss": 0.0, "inflow": 0.0, "state_of_charge_initial": 0.0,
-                    "cyclic_state_of_charge": False, "marginal_cost": 0.0, "marginal_cost_storage": 0.0,
-                    "spill_cost": 0.0, "state_of_charge_set": math.nan, "p_nom_extendable": False,
-                    "p_nom_min": 0.0, "p_nom_max": math.inf, "capital_cost": 0.0, "fom_cost": 0.0},
-    "Store": {"e_nom": 0.0, "e_min_pu": 0.0, "e_max_pu": 1.0, "e_initial": 0.0, "e_cyclic": False,
-              "standing_loss": 0.0, "marginal_cost": 0.0, "marginal_cost_storage": 0.0, "marginal_cost_quadratic": 0.0,
-              "p_set": math.nan, "e_set": math.nan, "e_nom_extendable": False, "e_nom_min": 0.0, "e_nom_max": math.inf,
-              "capital_cost": 0.0, "fom_cost": 0.0},
-    "GlobalConstraint": {"type": "primary_energy", "carrier_attribute": "co2_emissions", "sense": "=="},
-    "Carrier": {"co2_emissions": 0.0},
-}
+
+def _storage_type(pypsa_type: str) -> str:
+    """``AttributeType.parse`` (Schema.scala:20-37): the varying shapes
+    (``series``, ``static or series``, ``static``) are numbers."""
+    t = pypsa_type.strip().lower()
+    for kind, prefixes in (("float", ("float", "series", "static")), ("int", ("int",)), ("str", ("string",)),
+                           ("bool", ("bool",)), ("geometry", ("geometry",))):
+        if t.startswith(prefixes):
+            return kind
+    raise ValueError(f"unknown PyPSA attribute type '{pypsa_type}'")
+
+
+def _default_text(v) -> str:
+    """``Schema.renderDefault`` (Schema.scala:186-198): the schema tags
+    non-finite defaults rather than writing invalid JSON."""
+    if isinstance(v, bool):
+        return "true" if v else "false"
+    if isinstance(v, str):
+        return v
+    if v is None:
+        return ""
+    if isinstance(v, dict):
+        return "nan" if "$nan" in v else ("-inf" if v.get("$inf") == "-" else "inf")
+    if float(v) == math.floor(v) and abs(v) < 1e15:
+        return str(int(v))
+    return repr(float(v))
+
+
+def _typed_default(kind: str, text: str):
+    """A default as the column type stores it (CsvReader.scala:158-183,
+    :206-210): a float default that is absent or not a number is NaN, an
+    int's is 0, a boolean's false."""
+    if kind == "float":
+        if text in ("inf", "-inf", "nan"):
+            return {"inf": math.inf, "-inf": -math.inf, "nan": math.nan}[text]
+        v = _java_double(_java_trim(text)) if text else None
+        return math.nan if v is None else v
+    if kind == "int":
+        return int(text) if re.fullmatch(r"[+-]?\d+", text) else 0
+    if kind == "bool":
+        return text in ("true", "True")
+    return text
+
+
+def _load_schema():
+    with open(SCHEMA_FILE) as f:
+        raw = json.load(f)
+    list_names, attributes = {}, {}
+    for component, body in raw.items():
+        list_names[component] = body["list_name"]
+        attributes[component] = {}
+        for name, a in body["attributes"].items():
+            kind = _storage_type(a["type"])
+            default = _typed_default(kind, _default_text(a.get("default")))
+            attributes[component][name] = (kind, default)
+    return list_names, attributes
+
+
+# Java's String.trim and Double.parseDouble, which the reference's reader
+# applies to every cell: trim drops the characters up to U+0020 at either end;
+# the number grammar takes an optional sign, NaN, Infinity, decimal or
+# hexadecimal significands and a trailing type letter.
+_DECIMAL = re.compile(r"[+-]?(?:NaN|Infinity|(?:\d+\.?\d*|\.\d+)(?:[eE][+-]?\d+)?[fFdD]?)")
+_HEX = re.compile(r"([+-]?)0[xX]((?:[0-9a-fA-F]+\.?[0-9a-fA-F]*|\.[0-9a-fA-F]+)[pP][+-]?\d+)[fFdD]?")
+
+
+def _java_trim(text: str) -> str:
+    a, b = 0, len(text)
+    while a < b and text[a] <= " ":
+        a += 1
+    while b > a and text[b - 1] <= " ":
+        b -= 1
+    return text[a:b]
+
+
+def _java_double(text: str):
+    """``Double.parseDouble`` of a trimmed cell, or None where it throws."""
+    if _DECIMAL.fullmatch(text):
+        body = text.rstrip("fFdD") if text[-1] in "fFdD" else text
+        if body.lstrip("+-") == "NaN":
+            return math.nan
+        if body.lstrip("+-") == "Infinity":
+            return -math.inf if body[0] == "-" else math.inf
+        return float(body)
+    m = _HEX.fullmatch(text)
+    if m:
+        v = float.fromhex("0x" + m.group(2))
+        return -v if m.group(1) == "-" else v
+    return None
+
+
+LIST_NAMES, SCHEMA = _load_schema()  # component -> list name; component -> {attribute: (type, default)}
+COMPONENT_OF = {stem: component for component, stem in LIST_NAMES.items()}
+# the schema's defaults, which an omitted column or a blank cell resolves to
+DEFAULTS = {component: {a: d for a, (_, d) in attrs.items()} for component, attrs in SCHEMA.items()}
+PORT = re.compile(r"bus\d+")  # Topology.PortColumn: a bus name even when it reads as a number
 
 
 class MalformedNetwork(ValueError):
@@ -127,75 +191,211 @@ class Network:
         return 1.0 if w is None else float(w[t])
 
 
-# Attributes that name other entities or labels: kept as text even when they
-# read as numbers (bus "0" is a name, not a zero).
-LABELS = frozenset({"bus", "bus0", "bus1", "bus2", "bus3", "carrier", "control", "type", "sub_network",
-                    "generator", "country", "location", "unit", "sense", "investment_period", "mounting",
-                    "references", "model"})
+def split_line(line: str) -> list:
+    """``CsvReader.splitLine`` (CsvReader.scala:273-294): commas separate
+    fields, a double quote opens and closes a quoted stretch in which a
+    doubled quote is one quote and commas are text."""
+    if '"' not in line:
+        return line.split(",")
+    out, buf, quoted, i = [], [], False, 0
+    while i < len(line):
+        c = line[i]
+        if quoted:
+            if c == '"':
+                if i + 1 < len(line) and line[i + 1] == '"':
+                    buf.append('"')
+                    i += 1
+                else:
+                    quoted = False
+            else:
+                buf.append(c)
+        elif c == '"':
+            quoted = True
+        elif c == ",":
+            out.append("".join(buf))
+            buf = []
+        else:
+            buf.append(c)
+        i += 1
+    out.append("".join(buf))
+    return out
 
 
-def _coerce(v, label: bool = False):
-    """A cell: an empty one is absent (None: the attribute's default
-    applies), the text nan an explicit NaN (CsvReader.scala:150-221)."""
-    if v is None or (isinstance(v, float) and math.isnan(v)):
-        return None
-    if isinstance(v, str) and v.strip() == "":
-        return None
-    if label:
-        return str(v)
-    if isinstance(v, str):
-        t = v.strip()
-        if t.lower() in ("true", "false"):
-            return t.lower() == "true"
-        if t.lower() in ("nan", "na"):
-            return math.nan
-        try:
-            return float(t)
-        except ValueError:
-            return v
-    if isinstance(v, (bool, np.bool_)):
-        return bool(v)
-    return float(v)
+def _rows(path: str) -> list:
+    """The file's non-empty lines, split (CsvReader.parse, :263-271); a file
+    that is not there has none."""
+    if not os.path.exists(path):
+        return []
+    with open(path, encoding="utf-8", newline="") as f:  # lines end at LF, CR or CR LF only, as Java reads them
+        return [split_line(line) for line in re.split(r"\r\n|\r|\n", f.read()) if line]
 
 
-def read_table(path: str, component: str):
-    """One component list file (first column the names) as a Table of
-    static attributes, or None when it has no rows."""
-    df = pd.read_csv(path, dtype=str, keep_default_na=False)
-    if df.empty:
-        return None
-    ids = [str(v) for v in df[df.columns[0]]]
-    static = {col: {i: _coerce(v, col in LABELS or re.fullmatch(r"bus[0-9]+", col) is not None)
-                    for i, v in zip(ids, df[col])} for col in df.columns[1:]}
+def _number(cell: str, where: str) -> float:
+    """``CsvReader.parseFloat`` (CsvReader.scala:212-225): blank is NaN; a
+    cell Java cannot parse may still be inf, +inf, infinity, -inf,
+    -infinity, nan or na in any case; anything else is refused."""
+    t = _java_trim(cell)
+    if not t:
+        return math.nan
+    v = _java_double(t)
+    if v is not None:
+        return v
+    low = t.lower()
+    if low in ("inf", "+inf", "infinity"):
+        return math.inf
+    if low in ("-inf", "-infinity"):
+        return -math.inf
+    if low in ("nan", "na"):
+        return math.nan
+    raise MalformedNetwork(f"{where}: '{cell}' is not a number")
+
+
+def _java_int(t: str, default) -> int:
+    """``toIntOption``, else ``toDoubleOption`` cast to an Int (truncated,
+    saturating at the 32-bit range, NaN to 0), else the default."""
+    if re.fullmatch(r"[+-]?\d+", t) and -2**31 <= int(t) < 2**31:
+        return int(t)
+    v = _java_double(t)
+    if v is None:
+        return default
+    return 0 if math.isnan(v) else int(max(min(v, 2**31 - 1), -2**31))
+
+
+def _schema_column(kind: str, default, cells: list, where: str) -> list:
+    """A column the schema types (CsvReader.column, :146-183): a blank cell
+    takes the default, as an omitted column does."""
+    out = []
+    for c in cells:
+        t = _java_trim(c)
+        if not t:
+            out.append(default)
+        elif kind == "float":
+            out.append(_number(c, where))
+        elif kind == "int":
+            out.append(_java_int(t, default))
+        elif kind == "bool":
+            out.append(t.lower() in ("true", "1", "1.0"))
+        else:
+            out.append(t)
+    return out
+
+
+def _inferred_column(name: str, cells: list) -> list:
+    """A custom column (CsvReader.inferColumn, :191-204): a port holds bus
+    names; otherwise booleans if every present cell is True or False,
+    numbers (blank NaN) if every one parses, else text."""
+    trimmed = [_java_trim(c) for c in cells]
+    present = [t for t in trimmed if t]
+    if PORT.fullmatch(name):
+        return trimmed
+    if present and all(t in ("True", "False") for t in present):
+        return [t == "True" for t in trimmed]
+    if present:
+        parsed = [_java_double(t) if t else math.nan for t in trimmed]
+        if all(v is not None for v in parsed):
+            return parsed
+    return trimmed
+
+
+def _table_from_rows(rows: list, component: str) -> Table:
+    """``CsvReader.staticTable`` (:121-144): names in the first column."""
+    if not rows or not rows[0]:
+        return Table(component, [])
+    header, body = rows[0], rows[1:]
+    ids = [r[0] if r else "" for r in body]
+    attributes = SCHEMA.get(component, {})
+    list_name = LIST_NAMES.get(component, component)
+    static = {}
+    for k, name in enumerate(header[1:], start=1):
+        cells = [r[k] if k < len(r) else "" for r in body]
+        if name in attributes:
+            kind, default = attributes[name]
+            values = _schema_column(kind, default, cells, f"{list_name}.{name}")
+        else:
+            values = _inferred_column(name, cells)
+        static[name] = dict(zip(ids, values))
     return Table(component, ids, static)
 
 
+def read_table(path: str, component: str):
+    """One component list file as a Table of static attributes, or None
+    when it has no rows."""
+    table = _table_from_rows(_rows(path), component)
+    return table if len(table) else None
+
+
+def _snapshots(path: str):
+    """``CsvReader.readSnapshots`` (:87-107): labels from the column headed
+    snapshot, else the second; every other named column a weighting, a cell
+    that is not a number weighing 1."""
+    rows = _rows(path)
+    if not rows:
+        return [], {}
+    header, body = rows[0], rows[1:]
+    at = header.index("snapshot") if "snapshot" in header else (1 if len(header) > 1 else 0)
+    labels = [r[at] if at < len(r) else "" for r in body]
+    weightings = {}
+    for k, name in enumerate(header):
+        if k == at or not name:
+            continue
+        w = [_java_double(_java_trim(r[k])) if k < len(r) else None for r in body]
+        weightings[name] = np.array([1.0 if v is None else v for v in w], dtype=np.float64)
+    return labels, weightings
+
+
+_PLAIN = re.compile(r"[0-9eE+\-.,]*")  # cells Python and Java read alike
+
+
+def _series(path: str, snapshots: int, where: str):
+    """``CsvReader.readSeries`` (:227-261): the entities it covers and their
+    values [snapshots, entities]; one row per snapshot or the file is
+    refused."""
+    rows = _rows(path)
+    if not rows:
+        return [], np.zeros((snapshots, 0))
+    entities = [_java_trim(h) for h in rows[0][1:]]
+    body = rows[1:]
+    if len(body) != snapshots:
+        raise MalformedNetwork(f"{where} has {len(body)} rows but the network has {snapshots} snapshots")
+    values = np.empty((snapshots, len(entities)))
+    for t, r in enumerate(body):
+        cells = (r[1:] + [""] * len(entities))[:len(entities)]
+        if all(c and _PLAIN.fullmatch(c) for c in cells):
+            try:
+                values[t] = np.array(cells, dtype=np.float64)
+                continue
+            except ValueError:
+                pass  # a malformed number: the cell-by-cell path names it
+        values[t] = [_number(c, where) for c in cells]
+    return entities, values
+
+
 def read(folder: str, name: str = "") -> Network:
-    snap = pd.read_csv(os.path.join(folder, "snapshots.csv"))
-    label = "snapshot" if "snapshot" in snap.columns else snap.columns[0]
-    snapshots = list(snap[label])
-    weightings = {c: snap[c].to_numpy(dtype=np.float64) for c in ("objective", "stores", "generators")
-                  if c in snap.columns}
+    """``CsvReader.read`` (CsvReader.scala:34-75): the component tables the
+    schema names, each with its series files."""
+    if not os.path.isdir(folder):
+        raise MalformedNetwork(f"{folder} is not a directory")
+    csvs = sorted(f for f in os.listdir(folder) if f.endswith(".csv"))
+    snapshots, weightings = _snapshots(os.path.join(folder, "snapshots.csv"))
+    series_files: dict = {}
+    for f in csvs:
+        if "-" in f and f not in RESERVED:
+            stem = f[:-4]
+            series_files.setdefault(stem[:stem.index("-")], []).append(f)
     tables = {}
-    files = set(os.listdir(folder))
-    for component, stem in LIST_NAMES.items():
-        if f"{stem}.csv" not in files:
+    for f in csvs:
+        if "-" in f or f in RESERVED or f[:-4] not in COMPONENT_OF:
             continue
-        static_table = read_table(os.path.join(folder, f"{stem}.csv"), component)
-        if static_table is None:
-            continue
-        ids, static = static_table.ids, static_table.static
-        series = {}
-        for f in files:
-            if f.startswith(stem + "-") and f.endswith(".csv"):
-                attr = f[len(stem) + 1:-4]
-                s = pd.read_csv(os.path.join(folder, f), index_col=0)
-                arr = np.full((len(snapshots), len(ids)), math.nan)
-                for k, i in enumerate(ids):
-                    if i in s.columns:
-                        arr[:, k] = s[i].to_numpy(dtype=np.float64)
-                    else:
-                        arr[:, k] = float(Table(component, ids, static).value(attr, i))
-                series[attr] = arr
-        tables[component] = Table(component, ids, static, series)
+        component = COMPONENT_OF[f[:-4]]
+        table = _table_from_rows(_rows(os.path.join(folder, f)), component)
+        for sf in series_files.get(f[:-4], []):
+            attribute = sf[:-4].split("-", 1)[1]
+            entities, values = _series(os.path.join(folder, sf), len(snapshots), sf[:-4])
+            column = {e: k for k, e in enumerate(entities)}
+            arr = np.empty((len(snapshots), len(table.ids)))
+            for k, i in enumerate(table.ids):  # an entity the file does not cover keeps its static value
+                arr[:, k] = values[:, column[i]] if i in column else float(table.value(attribute, i))
+            table.series[attribute] = arr
+        if len(table):
+            tables[component] = table
     return Network(name or os.path.basename(folder.rstrip("/")), snapshots, weightings, tables)

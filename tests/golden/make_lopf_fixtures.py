@@ -1,5 +1,6 @@
-"""Copies PyPSA's standard type library into noaidi_b200/network/
-standard_types/, and the input tables of PyPSA golden networks and the expected LOPF
+"""Copies PyPSA's component schema (trimmed to list names, attribute types
+and defaults) into noaidi_b200/network/pypsa_schema.json, its standard type
+library into noaidi_b200/network/standard_types/, and the input tables of PyPSA golden networks and the expected LOPF
 results (objective, generator dispatch, line flows, storage trajectories,
 optimal capacities, the objective constant and PyPSA's branch outage
 distribution factors) from the reference's
@@ -58,6 +59,18 @@ def main(root):
     os.makedirs(library, exist_ok=True)
     for f in ("line_types.csv", "transformer_types.csv"):
         shutil.copyfile(os.path.join(goldens, "standard_types", f), os.path.join(library, f))
+    # PyPSA's component schema (list names, attribute types and defaults), which
+    # types every cell the network reader parses: package data too
+    schema = json.load(open(os.path.join(goldens, "schema.json")))
+    trimmed = {c: {"list_name": body["list_name"],
+                   "attributes": {a: {"type": v["type"], "default": v.get("default")}
+                                  for a, v in body["attributes"].items()}}
+               for c, body in sorted(schema.items())}
+    with open(os.path.join(os.path.dirname(library), "pypsa_schema.json"), "w") as f:  # an attribute per line
+        f.write("{\n" + ",\n".join(
+            f' {json.dumps(c)}: {{"list_name": {json.dumps(body["list_name"])}, "attributes": {{\n' +
+            ",\n".join(f"  {json.dumps(a)}: {json.dumps(v)}" for a, v in body["attributes"].items()) + "}}"
+            for c, body in trimmed.items()) + "\n}\n")
     for name in NETWORKS:
         src = os.path.join(goldens, "networks", name)
         dst = os.path.join(HERE, "lopf", name)
