@@ -194,6 +194,17 @@ class SparseMatrix:
         """``sqrt(||K||_1 ||K||_inf)`` (``SparseMatrix.scala:181``)."""
         return math.sqrt(self.norm1 * self.norm_inf)
 
+    def scaled_by(self, row_scale, col_scale) -> "SparseMatrix":
+        """diag(row_scale) A diag(col_scale) on the same pattern, each entry
+        (a * row) * col (``scaledBy``, SparseMatrix.scala:116-128)."""
+        rs = np.asarray(row_scale, dtype=np.float64)
+        cs = np.asarray(col_scale, dtype=np.float64)
+        _require(rs.shape == (self.rows,) and cs.shape == (self.cols,),
+                 f"scales have {rs.size} and {cs.size} entries for a {self.rows} x {self.cols} matrix")
+        rows_of = np.repeat(np.arange(self.rows), np.diff(self.row_ptr))
+        values = (self.values * rs[rows_of]) * cs[self.col_indices]
+        return SparseMatrix(self.rows, self.cols, self.row_ptr, self.col_indices, values)
+
     def to_dense(self) -> np.ndarray:
         out = np.zeros((self.rows, self.cols))
         rows_of = np.repeat(np.arange(self.rows), np.diff(self.row_ptr))

@@ -71,7 +71,61 @@ def test_vstack():
     assert list(s.multiply([1.0, 1.0])) == [3.0, 0.0, 0.0, 3.0]
 
 
+def test_transpose_round_trips_and_keeps_non_square_columns_ascending():
+    """SparseMatrixSuite.scala:26-48."""
+    d = SparseMatrix.from_dense([[1.0, 0.0, 2.0], [0.0, 3.0, 0.0], [4.0, 5.0, 6.0]], 3)
+    back = d.transpose.transpose
+    assert list(back.values) == list(d.values) and list(back.col_indices) == list(d.col_indices)
+    m = SparseMatrix.from_triplets(2, 4, [0, 0, 1, 1], [3, 1, 0, 3], [1.0, 2.0, 3.0, 4.0])
+    t = m.transpose
+    assert (t.rows, t.cols) == (4, 2)
+    for r in range(t.rows):
+        piece = list(t.col_indices[t.row_ptr[r]:t.row_ptr[r + 1]])
+        assert piece == sorted(piece)
+
+
+def test_multiply_agrees_with_the_dense_product_and_vstack_keeps_blocks():
+    """SparseMatrixSuite.scala:50-65: index-order sums, exact here."""
+    dense = [[1.0, 2.0, 0.0], [0.0, -1.0, 3.0]]
+    x = [2.0, 3.0, 4.0]
+    assert list(SparseMatrix.from_dense(dense, 3).multiply(x)) == [sum(a * b for a, b in zip(r, x)) for r in dense]
+    a = SparseMatrix.from_dense([[1.0, 2.0]], 2)
+    b = SparseMatrix.from_dense([[0.0, 3.0], [4.0, 0.0]], 2)
+    s = SparseMatrix.vstack([a, b])
+    assert (s.rows, s.nnz) == (3, 4) and s.to_dense().tolist() == [[1.0, 2.0], [0.0, 3.0], [4.0, 0.0]]
+
+
+def test_a_diagonal_has_equal_induced_norms_under_its_spectral_bound():
+    """SparseMatrixSuite.scala:82-98, the diagonal half."""
+    d = SparseMatrix.from_triplets(3, 3, [0, 1, 2], [0, 1, 2], [2.0, -7.0, 3.0])
+    assert d.norm1 == 7.0 and d.norm_inf == 7.0 and d.spectral_norm_bound >= 7.0 - 1e-12
+    col = SparseMatrix.from_triplets(25, 1, list(range(25)), [0] * 25, [1.0] * 25)
+    assert col.spectral_norm_bound > col.norm_inf
+
+
+def test_scaled_by_applies_row_and_column_diagonals():
+    """SparseMatrixSuite.scala:111-115."""
+    m = SparseMatrix.from_dense([[1.0, 2.0], [3.0, 4.0]], 2)
+    assert m.scaled_by([2.0, 10.0], [1.0, 0.5]).to_dense().tolist() == [[2.0, 2.0], [30.0, 20.0]]
+    with pytest.raises(ValueError):
+        m.scaled_by([1.0], [1.0, 1.0])
+
+
+def test_out_of_range_indices_are_refused_with_the_reference_message():
+    """SparseMatrixSuite.scala:117-121."""
+    with pytest.raises(ValueError, match=r"row index 2 out of range \[0, 2\)"):
+        SparseMatrix.from_triplets(2, 2, [2], [0], [1.0])
+
+
 # -- LpBuilderSuite.scala ------------------------------------------------------
+
+def test_duals_of_a_negated_row_come_back_with_the_callers_sign():
+    """LpBuilderSuite.scala:47-52."""
+    b = LpProblem.builder(1)
+    b.less_than([(0, 1.0)], 3.0)
+    _, t = b.build()
+    assert list(t.original_duals([2.0])) == [-2.0]
+
 
 def test_builder_orders_equalities_first():
     b = LpProblem.builder(2)
@@ -184,6 +238,14 @@ def test_scaled_optimum_stays_feasible_and_objective_invariant():
     assert np.allclose(ms.multiply(x), sq, atol=1e-8)
     assert np.all(x >= sl - 1e-9) and np.all(x <= su + 1e-9)
     assert float(sc @ x) == pytest.approx(float(p.objective @ np.array(inst.expected_primal)), abs=1e-8)
+
+
+def test_unscaling_recovers_the_original_coordinates():
+    """ScalingSuite.scala:31-40: x / colScale then * colScale."""
+    p = F.economic_dispatch().problem
+    *_, cs = O.scale(p)
+    point = 1.0 + 0.5 * np.arange(p.num_variables)
+    assert np.allclose((point / cs) * cs, point, rtol=0, atol=1e-12)
 
 
 # -- CertificatesSuite.scala ---------------------------------------------------
