@@ -1,9 +1,11 @@
 """Unit commitment (noaidi_b200/network/unit_commitment.py) on CPU, with the
 oracle solving every branch-and-bound node."""
+import os
+
 import pytest
 
 from noaidi_b200.network import unit_commitment as U
-from noaidi_b200.network.pypsa_csv import Table
+from noaidi_b200.network.pypsa_csv import Table, read
 from tests import bnb_fixtures as B
 from tests import uc_cases as X
 
@@ -42,4 +44,32 @@ def test_what_the_formulation_does_not_model_is_refused(mutate, word):
     n = X.network()
     mutate(n)
     with pytest.raises(U.UnsupportedNetwork, match=word):
+        U.build(n)
+
+
+def test_a_series_only_stand_by_cost_is_refused(tmp_path):
+    """UnitCommitmentSuite.scala:306-319: PyPSA writes the attribute as its
+    own file when only the series is non-default; there is no static column."""
+    import shutil
+    src = os.path.join(X.HERE, "unit-commitment")
+    for f in os.listdir(src):
+        shutil.copy(os.path.join(src, f), tmp_path / f)
+    (tmp_path / "generators-stand_by_cost.csv").write_text(
+        ",base\n0,0.0\n1,0.0\n2,25.0\n3,0.0\n4,0.0\n5,0.0\n6,0.0\n7,0.0\n")
+    n = read(str(tmp_path))
+    assert "stand_by_cost" not in n.table("Generator").static
+    with pytest.raises(U.UnsupportedNetwork, match="stand_by_cost"):
+        U.build(n)
+
+
+def test_a_priced_attribute_is_refused_even_with_no_snapshots(tmp_path):
+    """UnitCommitmentSuite.scala:321-344."""
+    (tmp_path / "buses.csv").write_text("name,v_nom,carrier\nbus,110.0,AC\n")
+    (tmp_path / "generators.csv").write_text("name,bus,p_nom,p_min_pu,marginal_cost,committable,stand_by_cost\n"
+                                             "unit,bus,100.0,0.5,10.0,True,25.0\n")
+    (tmp_path / "loads.csv").write_text("name,bus,p_set\nd,bus,50.0\n")
+    (tmp_path / "snapshots.csv").write_text(",snapshot\n")
+    n = read(str(tmp_path))
+    assert len(n.snapshots) == 0
+    with pytest.raises(U.UnsupportedNetwork, match="stand_by_cost"):
         U.build(n)
