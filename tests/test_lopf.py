@@ -642,6 +642,37 @@ def test_an_unrequested_bridge_column_is_marked_not_computed():
     assert not populated[at[("Line", "CD")]]
 
 
+def test_a_bridge_elsewhere_does_not_block_a_well_posed_contingency():
+    """SclopfSuite.scala:224-238: naming the spur is refused, an outage on
+    the triangle still builds its security rows."""
+    n = _triangle_with_spur()
+    with pytest.raises(lopf.UnsupportedNetwork, match="bridge"):
+        lopf.build_sclopf(n, [("Line", "CD")])
+    model = lopf.build_sclopf(n, [("Line", "AB")])
+    assert model.problem.num_constraints > lopf.build(n).problem.num_constraints
+
+
+def test_an_outage_naming_no_passive_branch_is_refused():
+    """SclopfSuite.scala:193-200."""
+    with pytest.raises(lopf.UnsupportedNetwork, match="nonexistent"):
+        lopf.build_sclopf(X.network("sclopf-triangle"), [("Line", "nonexistent")])
+
+
+def test_the_default_outage_set_is_every_passive_branch_and_security_costs_more():
+    """SclopfSuite.scala:81-98, :202-210: with no list every passive branch
+    is a contingency, which on the triangle is PyPSA's list, 14,100 against
+    the plain dispatch's 6,900."""
+    from oracle import oracle as O
+    n = X.network("sclopf-triangle")
+    exp = X.expected("sclopf-triangle")
+    assert sorted(exp["sclopf"]["branch_outages"]) == sorted(n.table("Line").ids)
+    secure = O.solve(lopf.build_sclopf(n).problem, X.PARAMS)
+    plain = O.solve(lopf.build(n).problem, X.PARAMS)
+    assert secure.objective_value == pytest.approx(14100.0, abs=1e-3)
+    assert plain.objective_value == pytest.approx(exp["objective"], abs=1e-3)
+    assert secure.objective_value > plain.objective_value + 1.0
+
+
 @pytest.mark.parametrize("ratio", [1e2, 1e4, 1e6])
 def test_factors_stay_bounded_near_a_bridge(tmp_path, ratio):
     """SclopfSuite.scala:395-424: a stiff branch beside a path ratio times
