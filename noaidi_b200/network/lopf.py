@@ -657,8 +657,11 @@ def solve(network: Network, params: PdhgParams = PdhgParams(), precision: int = 
           mixed: bool = False, ctx=None) -> LopfResult:
     """Build and solve on the GPU (``Lopf.solve``, :566-571); ``mixed`` runs
     the FP32 refinement scheme instead of plain FP64 PDHG."""
+    return _solve_model(network, build(network), params, precision, device, mixed, ctx)
+
+
+def _solve_model(network, model: Model, params, precision, device, mixed, ctx) -> LopfResult:
     from ..prima import cuda
-    model = build(network)
     if mixed:
         sol = cuda.mixed_solve(model.problem, params, ctx=ctx, device=device).solution
     else:
@@ -856,3 +859,11 @@ def build_sclopf(network: Network, outages: Optional[list] = None) -> Model:
     problem, translation = b.build()
     return Model(problem, translation, base.columns, base.balance_rows, base.cycles, base.objective_constant,
                  network)
+
+
+def solve_sclopf(network: Network, outages: Optional[list] = None, params: PdhgParams = PdhgParams(),
+                 precision: int = 64, device: int = 0, mixed: bool = False, ctx=None) -> LopfResult:
+    """Build the security-constrained LP and solve it on the GPU
+    (``Sclopf.solve``, Sclopf.scala:66-74); ``outages`` defaults to every
+    passive branch, and an empty list is the dispatch model."""
+    return _solve_model(network, build_sclopf(network, outages), params, precision, device, mixed, ctx)

@@ -787,3 +787,22 @@ def test_a_non_finite_factor_is_refused_for_a_requested_outage():
     [(carrier, buses, branches)] = lopf.sub_networks(n)
     with np.errstate(all="ignore"), pytest.raises(lopf.UnsupportedNetwork, match="non-finite"):
         lopf.lodf(n, carrier, buses, branches, {("Line", "AB")})
+
+
+def test_solve_sclopf_builds_the_secure_model_and_solves_it(monkeypatch):
+    """Sclopf.solve (Sclopf.scala:66-74): the device call is replaced by the
+    oracle here, so this checks which LP reaches it and what comes back."""
+    from noaidi_b200.prima import cuda
+    from oracle import oracle as O
+    seen = []
+
+    def fake_solve(problem, params, **kw):
+        seen.append(problem)
+        return O.solve(problem, params)
+    monkeypatch.setattr(cuda, "solve", fake_solve)
+    n = X.network("sclopf-triangle")
+    res = lopf.solve_sclopf(n, params=X.PARAMS)
+    assert res.objective == pytest.approx(14100.0, abs=1e-3)
+    assert seen[0].num_constraints == lopf.build_sclopf(n).problem.num_constraints
+    plain = lopf.solve_sclopf(n, [], params=X.PARAMS)
+    assert plain.objective == pytest.approx(6900.0, abs=1e-3)
