@@ -65,7 +65,7 @@ def _typed_default(kind: str, text: str):
         v = _java_double(_java_trim(text)) if text else None
         return math.nan if v is None else v
     if kind == "int":
-        return int(text) if re.fullmatch(r"[+-]?\d+", text) else 0
+        return int(text) if re.fullmatch(r"[+-]?[0-9]+", text) else 0
     if kind == "bool":
         return text in ("true", "True")
     return text
@@ -89,8 +89,8 @@ def _load_schema():
 # applies to every cell: trim drops the characters up to U+0020 at either end;
 # the number grammar takes an optional sign, NaN, Infinity, decimal or
 # hexadecimal significands and a trailing type letter.
-_DECIMAL = re.compile(r"[+-]?(?:NaN|Infinity|(?:\d+\.?\d*|\.\d+)(?:[eE][+-]?\d+)?[fFdD]?)")
-_HEX = re.compile(r"([+-]?)0[xX]((?:[0-9a-fA-F]+\.?[0-9a-fA-F]*|\.[0-9a-fA-F]+)[pP][+-]?\d+)[fFdD]?")
+_DECIMAL = re.compile(r"[+-]?(?:NaN|Infinity|(?:[0-9]+\.?[0-9]*|\.[0-9]+)(?:[eE][+-]?[0-9]+)?[fFdD]?)")
+_HEX = re.compile(r"([+-]?)0[xX]((?:[0-9a-fA-F]+\.?[0-9a-fA-F]*|\.[0-9a-fA-F]+)[pP][+-]?[0-9]+)[fFdD]?")
 
 
 def _java_trim(text: str) -> str:
@@ -122,7 +122,7 @@ LIST_NAMES, SCHEMA = _load_schema()  # component -> list name; component -> {att
 COMPONENT_OF = {stem: component for component, stem in LIST_NAMES.items()}
 # the schema's defaults, which an omitted column or a blank cell resolves to
 DEFAULTS = {component: {a: d for a, (_, d) in attrs.items()} for component, attrs in SCHEMA.items()}
-PORT = re.compile(r"bus\d+")  # Topology.PortColumn: a bus name even when it reads as a number
+PORT = re.compile(r"bus[0-9]+")  # Topology.PortColumn: a bus name even when it reads as a number
 
 
 class MalformedNetwork(ValueError):
@@ -253,7 +253,7 @@ def _number(cell: str, where: str) -> float:
 def _java_int(t: str, default) -> int:
     """``toIntOption``, else ``toDoubleOption`` cast to an Int (truncated,
     saturating at the 32-bit range, NaN to 0), else the default."""
-    if re.fullmatch(r"[+-]?\d+", t) and -2**31 <= int(t) < 2**31:
+    if re.fullmatch(r"[+-]?[0-9]+", t) and -2**31 <= int(t) < 2**31:
         return int(t)
     v = _java_double(t)
     if v is None:

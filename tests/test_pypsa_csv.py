@@ -192,3 +192,23 @@ def test_every_golden_network_reads_with_its_series_shaped_by_its_snapshots():
             for arr in tab.series.values():
                 assert arr.shape == (len(n.snapshots), len(tab.ids)), name
                 assert not np.isnan(arr).all() or len(tab.ids) == 0, name
+
+
+def test_the_number_grammar_agrees_with_the_oracles_restatement():
+    """Seeded random cells: the reader's parse (Java trim, then
+    Double.parseDouble) and the MPS oracle's independent restatement of the
+    same Java grammar accept the same strings with the same values --
+    including refusing digits outside ASCII, which Python's own float takes."""
+    from oracle.mps import java_double
+    rng = np.random.default_rng(7)
+    alphabet = list("0123456789+-.eExXpPfFdDaA ") + ["NaN", "Infinity", "0x", "١", "\t", "_"]
+    for _ in range(20000):
+        cell = "".join(rng.choice(alphabet, size=int(rng.integers(1, 9))))
+        ours = pypsa_csv._java_double(pypsa_csv._java_trim(cell)) if pypsa_csv._java_trim(cell) else None
+        theirs = java_double(cell) if cell.strip("".join(chr(i) for i in range(0x21))) else None
+        if theirs is None or ours is None:
+            assert ours is None and theirs is None, repr(cell)
+        else:
+            assert (math.isnan(ours) and math.isnan(theirs)) or ours == theirs, repr(cell)
+    with pytest.raises(MalformedNetwork):
+        pypsa_csv._number("١٢", "buses.v_nom")
