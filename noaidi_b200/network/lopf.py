@@ -267,6 +267,38 @@ def dangling_bus_references(network: Network) -> list:
     return out
 
 
+def _pairs(network: Network, components) -> list:
+    """``Topology.branchesWhere`` (Topology.scala:234-252): every pair of a
+    branch's non-blank ports, so a multi-port link connects all of them."""
+    out = []
+    for comp in components:
+        tab = network.table(comp)
+        ports = _ports(network, comp)
+        for i in tab.ids:
+            ends = [b for b in (tab.endpoint(p, i) for p in ports) if b]
+            out += [(a, b) for k, a in enumerate(ends) for b in ends[k + 1:]]
+    return out
+
+
+def controllable_branches(network: Network) -> list:
+    """Endpoint pairs of the links (``Topology.controllableBranches``)."""
+    return _pairs(network, ("Link",))
+
+
+def isolated_buses(network: Network) -> list:
+    """Buses no branch of any kind reaches (``Topology.isolatedBuses``,
+    Topology.scala:335-344): a load there makes the network infeasible."""
+    connected = {b for pair in _pairs(network, BRANCHES) for b in pair}
+    return [b for b in network.table("Bus").ids if b not in connected]
+
+
+def attached_to(network: Network, bus: str) -> list:
+    """(component, id) of the one-ports at a bus (``Topology.attachedTo``);
+    branches are not attached, they have bus0 and bus1."""
+    return [(comp, i) for comp in ONE_PORTS for i in network.table(comp).ids
+            if network.table(comp).endpoint("bus", i) == bus]
+
+
 def link_ports(links) -> list:
     """``Topology.portsOf``: bus0, bus1 and any further busN columns of the
     links, in port order (a multi-port link, PyPSA's ``bus2``...)."""

@@ -1,7 +1,8 @@
 """Sub-network decomposition and bus references (``Topology``,
 modules/network-model/src/main/scala/org/noaidi/network/Topology.scala), with
-the cases of TopologySuite.scala that apply to the LOPF builders.  Networks
-written here go through the CSV reader, where column typing happens."""
+the cases of TopologySuite.scala (all but the schema-role one, which concerns
+the reference's component registry).  Networks written here go through the
+CSV reader, where column typing happens."""
 import pytest
 
 from noaidi_b200.network import lopf
@@ -181,3 +182,40 @@ def test_the_dispatch_model_refuses_a_reference_to_no_bus(tmp_path, table, row):
     (tmp_path / "bad").mkdir()
     with pytest.raises(lopf.UnsupportedNetwork, match="unknown bus"):
         lopf.build(_via_reader(tmp_path / "bad", files))
+
+
+def test_a_multi_port_branch_connects_all_of_its_ports(tmp_path):
+    """TopologySuite.scala:144-195: every pair, so connectivity over the link
+    is transitive, and the third port is not isolated."""
+    n = _via_reader(tmp_path, {"buses.csv": "name,v_nom,carrier\na,380.0,AC\nb,380.0,AC\nc,380.0,AC\n",
+                               "links.csv": "name,bus0,bus1,bus2\nk,a,b,c\n"})
+    assert lopf.link_ports(n.table("Link")) == ["bus0", "bus1", "bus2"]
+    assert len(lopf.controllable_branches(n)) == 3
+    assert lopf.isolated_buses(n) == []
+
+
+def test_attached_components_are_found_by_their_bus():
+    """TopologySuite.scala:322-333."""
+    n = X.network("ac-dc-meshed")
+    at = lopf.attached_to(n, "Manchester")
+    assert at and all(n.table(c).endpoint("bus", i) == "Manchester" for c, i in at)
+    assert not any(c in ("Line", "Link") for c, _ in at)
+
+
+def test_an_isolated_bus_is_reported(tmp_path):
+    """TopologySuite.scala:335-345."""
+    n = _via_reader(tmp_path, {"buses.csv": "name\nconnected0\nconnected1\nnowhere\n",
+                               "lines.csv": "name,bus0,bus1\nl0,connected0,connected1\n"})
+    assert lopf.isolated_buses(n) == ["nowhere"]
+
+
+def test_no_golden_network_with_branches_has_an_isolated_bus():
+    """TopologySuite.scala:347-373: unit-commitment, one bus and no
+    branches, is the degenerate shape and is excluded."""
+    with_branches = [name for name in X.NETWORKS
+                     if lopf.passive_branches(X.network(name)) or lopf.controllable_branches(X.network(name))]
+    assert len(with_branches) >= 5
+    for name in with_branches:
+        assert lopf.isolated_buses(X.network(name)) == [], name
+    single = X.network("unit-commitment")
+    assert len(single.table("Bus")) == 1 and lopf.passive_branches(single) == []
