@@ -64,11 +64,21 @@ import numpy as np
 from ..prima.model import LpBuilder, LpProblem, Negated, RowTranslation
 from ..prima.types import LpSolution, PdhgParams, SolveStatus
 from . import standard_types
-from .pypsa_csv import LIST_NAMES, MalformedNetwork, Network
+from .pypsa_csv import CATEGORY, LIST_NAMES, MalformedNetwork, Network
 
 HANDLED = {"Bus", "Carrier", "Generator", "Load", "Line", "Transformer", "Link", "GlobalConstraint", "SubNetwork",
            "LineType", "TransformerType", "Shape", "StorageUnit", "Store"}
-PASSIVE = ("Line", "Transformer")  # branches whose flow follows from impedance
+
+
+def _role(*categories) -> tuple:
+    """Components by PyPSA's own category (``Role.of``, Topology.scala:31-49),
+    in the order of their list names, as the reference reads the files."""
+    return tuple(sorted((c for c, k in CATEGORY.items() if k in categories), key=LIST_NAMES.get))
+
+
+PASSIVE = _role("passive_branch")  # Line, Transformer: branches whose flow follows from impedance
+BRANCHES = _role("passive_branch", "controllable_branch")  # with Link and Process
+ONE_PORTS = _role("controllable_one_port", "passive_one_port")  # attached at one bus
 
 
 class UnsupportedNetwork(ValueError):
@@ -221,8 +231,6 @@ def _reject(network: Network) -> None:
         raise UnsupportedNetwork(f"{comp} '{i}' references unknown bus '{bus}' via {port}")
 
 
-BRANCHES = PASSIVE + ("Link",)
-ONE_PORTS = ("Generator", "Load", "StorageUnit", "Store")
 
 
 def _ports(network: Network, component: str) -> list:
@@ -235,7 +243,7 @@ def _ports(network: Network, component: str) -> list:
         if required not in tab.static:
             raise MalformedNetwork(f"{LIST_NAMES[component]} has no '{required}' column; a branch needs both "
                                    "endpoints")
-    return link_ports(tab) if component == "Link" else ["bus0", "bus1"]
+    return link_ports(tab)
 
 
 def dangling_references(network: Network, components=BRANCHES) -> list:
@@ -281,8 +289,9 @@ def _pairs(network: Network, components) -> list:
 
 
 def controllable_branches(network: Network) -> list:
-    """Endpoint pairs of the links (``Topology.controllableBranches``)."""
-    return _pairs(network, ("Link",))
+    """Endpoint pairs of the links and processes
+    (``Topology.controllableBranches``)."""
+    return _pairs(network, _role("controllable_branch"))
 
 
 def isolated_buses(network: Network) -> list:
@@ -300,8 +309,8 @@ def attached_to(network: Network, bus: str) -> list:
 
 
 def link_ports(links) -> list:
-    """``Topology.portsOf``: bus0, bus1 and any further busN columns of the
-    links, in port order (a multi-port link, PyPSA's ``bus2``...)."""
+    """``Topology.portsOf``: bus0, bus1 and any further busN columns of a
+    branch table, in port order (a multi-port link, PyPSA's ``bus2``...)."""
     ports = [c for c in links.static if re.fullmatch(r"bus[0-9]+", c)]
     return sorted(set(ports) | {"bus0", "bus1"}, key=lambda c: int(c[3:]))
 
@@ -560,9 +569,9 @@ def build(network: Network) -> Model:
         attached[str(stores.value("bus", s_))]["store"].append(s_)
     for d in loads.ids:
         attached[str(loads.value("bus", d))]["load"].append(d)
-    for comp in BRANCHES:
+    for comp in PASSIVE + ("Link",):  # the branches the model builds (a process is refused)
         tab = network.table(comp)
-        ports = _ports(network, comp)
+        ports = link_ports(tab) if comp == "Link" else ["bus0", "bus1"]  # a line's flow has two ends
         for e in tab.ids:  # bus0 first, so a branch looping onto one bus lists -1 then its efficiency
             for port in ports:
                 bus = tab.endpoint(port, e)  # '' for a port this link leaves unconnected

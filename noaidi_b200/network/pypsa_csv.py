@@ -74,15 +74,16 @@ def _typed_default(kind: str, text: str):
 def _load_schema():
     with open(SCHEMA_FILE) as f:
         raw = json.load(f)
-    list_names, attributes = {}, {}
+    list_names, categories, attributes = {}, {}, {}
     for component, body in raw.items():
         list_names[component] = body["list_name"]
+        categories[component] = body.get("category") or ""
         attributes[component] = {}
         for name, a in body["attributes"].items():
             kind = _storage_type(a["type"])
             default = _typed_default(kind, _default_text(a.get("default")))
             attributes[component][name] = (kind, default)
-    return list_names, attributes
+    return list_names, categories, attributes
 
 
 # Java's String.trim and Double.parseDouble, which the reference's reader
@@ -118,7 +119,8 @@ def _java_double(text: str):
     return None
 
 
-LIST_NAMES, SCHEMA = _load_schema()  # component -> list name; component -> {attribute: (type, default)}
+# component -> list name; -> PyPSA category (passive_branch, controllable_one_port, ...); -> {attribute: (type, default)}
+LIST_NAMES, CATEGORY, SCHEMA = _load_schema()
 COMPONENT_OF = {stem: component for component, stem in LIST_NAMES.items()}
 # the schema's defaults, which an omitted column or a blank cell resolves to
 DEFAULTS = {component: {a: d for a, (_, d) in attrs.items()} for component, attrs in SCHEMA.items()}

@@ -1,9 +1,9 @@
-"""Copies PyPSA's component schema (trimmed to list names, attribute types
-and defaults) into noaidi_b200/network/pypsa_schema.json, its standard type
+"""Copies PyPSA's component schema (trimmed to list names, categories,
+attribute types and defaults) into noaidi_b200/network/pypsa_schema.json, its standard type
 library into noaidi_b200/network/standard_types/, and the input tables of PyPSA golden networks and the expected LOPF
 results (objective, generator dispatch, line flows, storage trajectories,
-optimal capacities, the objective constant and PyPSA's branch outage
-distribution factors) from the reference's
+optimal capacities, the objective constant, PyPSA's branch outage
+distribution factors and its island split) from the reference's
 goldens (reference/goldens/{networks,results} in oluies/noaidi, generated by
 PyPSA 1.2.4) into tests/golden/lopf/<network>/.
 
@@ -62,15 +62,17 @@ def main(root):
     # PyPSA's component schema (list names, attribute types and defaults), which
     # types every cell the network reader parses: package data too
     schema = json.load(open(os.path.join(goldens, "schema.json")))
-    trimmed = {c: {"list_name": body["list_name"],
+    trimmed = {c: {"list_name": body["list_name"], "category": body.get("category"),
                    "attributes": {a: {"type": v["type"], "default": v.get("default")}
                                   for a, v in body["attributes"].items()}}
                for c, body in sorted(schema.items())}
     with open(os.path.join(os.path.dirname(library), "pypsa_schema.json"), "w") as f:  # an attribute per line
         f.write("{\n" + ",\n".join(
-            f' {json.dumps(c)}: {{"list_name": {json.dumps(body["list_name"])}, "attributes": {{\n' +
+            f' {json.dumps(c)}: {{"list_name": {json.dumps(body["list_name"])}, '
+            f'"category": {json.dumps(body["category"])}, "attributes": {{\n' +
             ",\n".join(f"  {json.dumps(a)}: {json.dumps(v)}" for a, v in body["attributes"].items()) + "}}"
             for c, body in trimmed.items()) + "\n}\n")
+    manifest = json.load(open(os.path.join(goldens, "manifest.json")))["networks"]
     for name in NETWORKS:
         src = os.path.join(goldens, "networks", name)
         dst = os.path.join(HERE, "lopf", name)
@@ -79,9 +81,11 @@ def main(root):
             if os.path.exists(os.path.join(src, f)):
                 _copy_table(os.path.join(src, f), os.path.join(dst, f))
         results = os.path.join(goldens, "results", f"{name}.json")
+        # PyPSA's own island split (determine_network_topology), as carrier and buses
+        islands = [{"carrier": sn["carrier"], "buses": sn["buses"]} for sn in manifest[name]["sub_networks"]]
         if not os.path.exists(results):  # no results file: the optimum PyPSA's run recorded, if any
             with open(os.path.join(dst, "expected.json"), "w") as f:
-                json.dump(RECORDED[name], f, indent=1)
+                json.dump({**RECORDED[name], "sub_networks": islands}, f, indent=1)
             print(name, "->", dst, "(recorded objective)")
             continue
         full = json.load(open(results))
@@ -95,6 +99,7 @@ def main(root):
                                                              "line_p0")}
         if isinstance(full.get("bodf"), dict) and "error" not in full["bodf"]:  # PyPSA's BODF per sub-network
             keep["bodf"] = full["bodf"]
+        keep["sub_networks"] = islands
         with open(os.path.join(dst, "expected.json"), "w") as f:
             json.dump(keep, f, indent=1)
         print(name, "->", dst)

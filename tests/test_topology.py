@@ -219,3 +219,24 @@ def test_no_golden_network_with_branches_has_an_isolated_bus():
         assert lopf.isolated_buses(X.network(name)) == [], name
     single = X.network("unit-commitment")
     assert len(single.table("Bus")) == 1 and lopf.passive_branches(single) == []
+
+
+def test_component_roles_come_from_pypsas_category():
+    """TopologySuite.scala:31-45: Process is a second controllable branch
+    and a shunt an attached one-port without either being named."""
+    assert lopf.PASSIVE == ("Line", "Transformer")
+    assert set(lopf.BRANCHES) - set(lopf.PASSIVE) == {"Link", "Process"}
+    assert {"Generator", "Load", "ShuntImpedance", "StorageUnit", "Store"} == set(lopf.ONE_PORTS)
+    assert not {"Bus", "Carrier", "LineType"} & set(lopf.BRANCHES + lopf.ONE_PORTS)
+
+
+@pytest.mark.parametrize("name", X.NETWORKS)
+def test_each_golden_network_decomposes_into_pypsas_sub_networks(name):
+    """TopologySuite.scala:57-82: the islands PyPSA's
+    determine_network_topology found, as a set (PyPSA numbers them its own
+    way), and ours in order of their first bus."""
+    expected = {(sn["carrier"], tuple(sorted(sn["buses"]))) for sn in X.expected(name)["sub_networks"]}
+    actual = [(s.carrier, tuple(s.buses)) for s in lopf.sub_networks(X.network(name))]
+    assert len(actual) == len(expected) and set(actual) == expected
+    heads = [b[0] for _, b in actual]
+    assert heads == sorted(heads)
