@@ -775,7 +775,46 @@ def sub_networks(network: Network) -> list:
     return out
 
 
-def lodf(network: Network, carrier: str, buses: list, branches: list, outages: Optional[set] = None):
+class Lodf(tuple):
+    """Outage factors of one sub-network (``Lodf``, Lodf.scala:14-66);
+    unpacks as (branches, factors, populated).  ``factor(affected, outage)``
+    is the share of the outaged branch's flow that reappears on the affected
+    one."""
+
+    def __new__(cls, branches: list, factors: np.ndarray, populated: np.ndarray):
+        self = super().__new__(cls, (branches, factors, populated))
+        self.index = {b: k for k, b in enumerate(branches)}
+        return self
+
+    branches = property(lambda self: self[0])
+
+    def __contains__(self, branch) -> bool:
+        return branch in self.index
+
+    def _column(self, outage) -> int:
+        j = self.index[outage]
+        if not self[2][j]:
+            raise KeyError(f"the outage column for {outage} was not computed: it was not among the requested "
+                           "contingencies, so its factors were never validated")
+        return j
+
+    def factor(self, affected, outage) -> float:
+        """Refuses a branch this sub-network does not hold, and a column that
+        was never computed: neither is a zero."""
+        for b in (affected, outage):
+            if b not in self.index:
+                raise KeyError(f"no branch {b} here")
+        return float(self[1][self.index[affected], self._column(outage)])
+
+    def factor_or_zero(self, affected, outage) -> float:
+        """As ``factor``, but zero when either branch is in another
+        sub-network, which is physically zero (``factorOrZero``)."""
+        if affected not in self.index or outage not in self.index:
+            return 0.0
+        return float(self[1][self.index[affected], self._column(outage)])
+
+
+def lodf(network: Network, carrier: str, buses: list, branches: list, outages: Optional[set] = None) -> Lodf:
     """Branch outage distribution factors of one sub-network (``Lodf.of``,
     modules/network-pf/.../Lodf.scala): PTDF = diag(b) A B^-1 with the first
     bus as reference (the factors do not depend on that choice), and
@@ -784,11 +823,11 @@ def lodf(network: Network, carrier: str, buses: list, branches: list, outages: O
     has no post-outage flow: it is refused if requested as a contingency and
     left unpopulated otherwise; a requested column with a non-finite factor
     is refused too (Lodf.scala:187-230).  ``branches`` are
-    (component, id) keys.  Returns (branches, factors m x m, populated per
-    outage column)."""
+    (component, id) keys.  Returns a ``Lodf``: (branches, factors m x m,
+    populated per outage column), read by branch with ``factor``."""
     m = len(branches)
     if m == 0:
-        return [], np.zeros((0, 0)), np.zeros(0, dtype=bool)
+        return Lodf([], np.zeros((0, 0)), np.zeros(0, dtype=bool))
     index = {b: i for i, b in enumerate(buses[1:])}
     n = len(index)
     y = np.array([susceptance(network, c, i, carrier) for c, i in branches])
@@ -823,7 +862,7 @@ def lodf(network: Network, carrier: str, buses: list, branches: list, outages: O
         if requested and not np.isfinite(factors[:, j]).all():
             raise UnsupportedNetwork(f"outage of {key[0]} '{key[1]}' gives a non-finite factor, so its "
                                      "sub-network's susceptance matrix did not solve cleanly")
-    return branches, factors, populated
+    return Lodf(list(branches), factors, populated)
 
 
 def _outage_key(network: Network, o) -> tuple:

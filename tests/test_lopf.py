@@ -806,3 +806,21 @@ def test_solve_sclopf_builds_the_secure_model_and_solves_it(monkeypatch):
     assert seen[0].num_constraints == lopf.build_sclopf(n).problem.num_constraints
     plain = lopf.solve_sclopf(n, [], params=X.PARAMS)
     assert plain.objective == pytest.approx(6900.0, abs=1e-3)
+
+
+def test_a_factor_is_read_by_branch_and_refuses_what_was_not_computed():
+    """Lodf.factor / factorOrZero (Lodf.scala:40-66): an unknown branch and an
+    uncomputed column are errors; only another sub-network is a zero."""
+    n = _triangle_with_spur()
+    [(carrier, buses, branches)] = lopf.sub_networks(n)
+    f = lopf.lodf(n, carrier, buses, branches, {("Line", "AB")})
+    assert ("Line", "AB") in f and ("Line", "XY") not in f
+    assert abs(f.factor(("Line", "BC"), ("Line", "AB"))) == pytest.approx(1.0, abs=1e-9)
+    assert f.factor(("Line", "AB"), ("Line", "AB")) == -1.0
+    with pytest.raises(KeyError, match="not computed"):
+        f.factor(("Line", "AB"), ("Line", "CD"))
+    with pytest.raises(KeyError, match="not computed"):
+        f.factor_or_zero(("Line", "AB"), ("Line", "CD"))
+    with pytest.raises(KeyError, match="no branch"):
+        f.factor(("Line", "AB"), ("Line", "typo"))
+    assert f.factor_or_zero(("Line", "AB"), ("Line", "elsewhere")) == 0.0
