@@ -14,16 +14,23 @@ value   whole-job LPs/s; each step is one prima_problem_mixed_solve on a
         CUDA events on the library's stream; max over ranks.
 e2e     the same metric through the one-shot C-ABI call with host buffers
         (upload, device equilibration, both passes, download of x, y and the
-        reduced costs inside the timed region).
+        reduced costs inside the timed region), on the first --e2e-steps steps.
 fp64    plain FP64 device PDHG (the reference algorithm, ScalaKernels
-        semantics): its per-iteration cost is measured on a bounded run and
-        its time to 1e-8 is that cost times the iteration count the full FP64
-        solve of this instance needs (FP64_ITERATIONS_TO_TOLERANCE, measured
-        on a B200 with --full-fp64, which reruns it).
+        semantics) on the same instance, solved to the same tolerance in full
+        once per run: its time, iteration count, status and objective.
+error   the refinement's objective against that FP64 answer and against
+        HiGHS's optimum of the instance (tests/golden/bench_highs.json, made
+        by tests/golden/make_bench_fixtures.py).
+batch   (--batch K, 256 by default) the uneven sweep of K DC-LOPF instances,
+        FP32 refinement to 1e-6, one launch per pass: LPs/s, its own
+        roofline, a CPU estimate and errors against HiGHS on a sample.
+config1 the 600-column random sparse LP solved to 1e-6 by the device and by
+        the oracle on a host core, both measured in full.
 
 ``--impl reference`` times the CPU restatement of the reference FP64 PDHG
 (single-threaded, like the reference's ScalaKernels backend) on a bounded
-sample of the same instance on the host cores, rank 0 only.
+sample of the same instance on the host cores, rank 0 only, and solves the
+600-column LP to tolerance in full.
 """
 from __future__ import annotations
 
@@ -45,11 +52,17 @@ UNIT = "LPs/s"
 EPS = 1e-8
 WORKLOAD = dict(buses=2000, lines=3000, generators=1000, snapshots=168)
 WORKLOAD_NAME = "dc-lopf-2000bus-3000line-1000gen-168h (n=1,344,000 m=840,000 nnz=3,024,000)"
-# Iterations the plain FP64 device PDHG needs to reach 1e-8 on the seed-0
-# instance, from a full run (python bench.py --full-fp64); the CPU baseline
-# uses the same count.
+# Iterations the plain FP64 device PDHG needed to reach 1e-8 on the seed-0
+# instance in a full solve (the default run measures it again and reports the
+# count it saw); only the reference arm, which runs without a GPU, uses this.
 FP64_ITERATIONS_TO_TOLERANCE = 1_216_064
 ROUND_REDUCTION = 10.0
+BATCH_EPS = 1e-6
+CONFIG1 = dict(m=400, n=600, per_column=5)
+CONFIG1_EPS = 1e-6
+# DRAM bytes (read + write) per step-size trial of pdhg_kernel<float> on this
+# workload, from an ncu capture of a bounded run of the same instance.
+TRAFFIC_BYTES_PER_TRIAL = 140.5e6
 
 
 def peaks():
@@ -57,6 +70,18 @@ def peaks():
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "MEASURED_PEAKS.json hbm_gbs"
     except Exception:
         return {"hbm_gbs": 6650.0}, "fallback 6.65 TB/s"
+
+
+def host_info():
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"host_cores": os.cpu_count(), "cpu_model": model}
 
 
 class ClockSampler:
@@ -124,6 +149,33 @@ def algorithmic_bytes(problem, trials: int, iterations: int, word: int, anchored
     return acc * iterations + rej * max(0, trials - iterations)
 
 
+def bench_config(problem, eps, world, round_reduction):
+    K = problem.constraint_matrix
+    return {"workload": WORKLOAD_NAME, "n": problem.num_variables, "m": problem.num_constraints, "nnz": int(K.nnz),
+            "eps": eps, "seed": "rank", "parallelism": f"independent instances x{world}",
+            "scheme": f"fp32 pass + fp32 refinement around an fp64 anchor, round reduction {round_reduction:g}",
+            "l2": "working set larger than L2 (no flush needed)"}
+
+
+def highs_reference(seed, problem):
+    """HiGHS's optimum of the bench instance with this seed, if recorded for
+    exactly these bytes."""
+    from noaidi_b200.prima.generators import problem_hash
+    try:
+        rec = json.load(open(os.path.join(ROOT, "tests", "golden", "bench_highs.json"))).get(str(seed))
+    except (OSError, ValueError):
+        return None
+    if not rec or rec.get("hash") != problem_hash(problem):
+        return None
+    return float(rec["highs_objective"])
+
+
+def rel_err(a, b):
+    return None if a is None or b is None else abs(a - b) / max(1.0, abs(b))
+
+
+# ---- CPU legs (the oracle: test infrastructure, timed as the CPU baseline) ----
+
 def cpu_sample(problem, iters: int, repeats: int = 1):
     """The oracle (reference FP64 PDHG restated in C, one thread) for a fixed
     number of iterations: seconds per iteration, setup (equilibration) taken
@@ -142,8 +194,27 @@ def cpu_sample(problem, iters: int, repeats: int = 1):
     return float(np.median(times)), s.iterations
 
 
+def config1_problem():
+    from noaidi_b200.prima import generators as G
+    return G.random_sparse_lp(seed=0, **CONFIG1)
+
+
+def config1_oracle():
+    """The 600-column LP solved to 1e-6 by the oracle on one host core, in full."""
+    from noaidi_b200.prima import PdhgParams
+    from oracle import oracle as O
+    p = config1_problem()
+    params = PdhgParams(eps_abs=CONFIG1_EPS, eps_rel=CONFIG1_EPS, max_iterations=1_000_000)
+    O.solve(p, params.copy(max_iterations=64))  # warm the library
+    t = time.perf_counter()
+    s = O.solve(p, params)
+    secs = time.perf_counter() - t
+    return {"seconds": secs, "iterations": s.iterations, "status": s.status.name, "objective": s.objective_value}
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     from noaidi_b200.prima import generators as G
@@ -151,35 +222,27 @@ def run_reference(args) -> None:
     for _ in range(min(args.warmup, 1)):
         cpu_sample(problem, 1)
     per_iter, done = cpu_sample(problem, args.cpu_sample_iterations, args.steps)
-    iters = FP64_ITERATIONS_TO_TOLERANCE or args.fp64_iterations
+    iters = FP64_ITERATIONS_TO_TOLERANCE
     lps = 1.0 / (per_iter * iters)
+    hi = host_info()
+    c1 = config1_oracle()
     line = {"impl": "reference", "metric": METRIC, "value": lps, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / lps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "eps": EPS, "seed": 0},
-            "cpu_baseline": {"value": lps, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": f"{done} FP64 PDHG iterations per step of the same instance "
-                                       f"(oracle restatement of Pdhg.Solve + ScalaKernels, 1 thread, like the "
-                                       f"reference); {per_iter * 1e3:.1f} ms/iteration extrapolated to the "
-                                       f"{iters} iterations the FP64 solve needs to 1e-8"},
-            "e2e": {"value": lps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": bench_config(problem, EPS, world, args.round_reduction),
+            "cpu_baseline": {"value": lps, "unit": UNIT, "cores": 1, **hi, "kind": "port", "extrapolated": True,
+                             "sample": f"EXTRAPOLATED, not solved: {done} FP64 PDHG iterations per step of the seed-0 "
+                                       f"instance on one host core (the oracle, Pdhg.Solve + ScalaKernels restated "
+                                       f"in C, single-threaded like the reference), {per_iter * 1e3:.1f} "
+                                       f"ms/iteration, times the {iters} iterations the same algorithm needed on the "
+                                       f"device in FP64 to reach 1e-8 (a full run of that solve on the CPU would "
+                                       f"take about {per_iter * iters / 3600:.1f} h)"},
+            "e2e": {"value": lps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "config1_measured": {"workload": "random sparse LP m=400 n=600 (5 nonzeros per column), seed 0",
+                                 "eps": CONFIG1_EPS, "cores": 1, "time_to_tolerance_s": c1["seconds"],
+                                 "iterations": c1["iterations"], "status": c1["status"],
+                                 "objective": c1["objective"], "lps_per_s": 1.0 / c1["seconds"]}}
     print(json.dumps(line), flush=True)
-
-
-BATCH_EPS = 1e-6
-
-
-def _batch_specs(seed: int, count: int, min_buses=100, max_buses=2000, min_snapshots=24, max_snapshots=168):
-    """The (seed, buses, lines, generators, snapshots, load scale) of each
-    instance of ``generators.lopf_batch``, drawn the same way."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for i in range(count):
-        B = int(rng.integers(min_buses, max_buses + 1))
-        T = int(rng.integers(min_snapshots, max_snapshots + 1))
-        scale = float(rng.uniform(0.6, 0.95))
-        out.append((seed + i, B, (3 * B) // 2, B // 2, T, scale))
-    return out
 
 
 def _oracle_seconds_per_iteration(spec, iters: int = 16) -> float:
@@ -196,7 +259,29 @@ def _oracle_seconds_per_iteration(spec, iters: int = 16) -> float:
     return max(time.perf_counter() - t - t1, 1e-9) / max(1, s.iterations - 1)
 
 
-def batch_cpu_baseline(specs, nnz, iterations, sample: int = 8):
+def _batch_specs(seed: int, count: int, min_buses=100, max_buses=2000, min_snapshots=24, max_snapshots=168):
+    """The (seed, buses, lines, generators, snapshots, load scale) of each
+    instance of ``generators.lopf_batch``, drawn the same way."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        B = int(rng.integers(min_buses, max_buses + 1))
+        T = int(rng.integers(min_snapshots, max_snapshots + 1))
+        scale = float(rng.uniform(0.6, 0.95))
+        out.append((seed + i, B, (3 * B) // 2, B // 2, T, scale))
+    return out
+
+
+def _highs_lopf(spec):
+    """HiGHS's optimum of one batch instance, snapshot by snapshot (nothing
+    couples the snapshots of a dispatch LP)."""
+    from noaidi_b200.prima import generators as G
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_bench_fixtures import highs_by_snapshot
+    return highs_by_snapshot(G.dc_lopf(*spec), spec[4])
+
+
+def batch_cpu_baseline(pool, specs, nnz, iterations, sample: int = 8):
     """``PrimaZio.solveAll``'s CPU shape -- one single-threaded FP64 solve per
     host core at a time -- estimated from a bounded sample: up to ``sample``
     instances spread over the sizes are timed per iteration in parallel
@@ -204,59 +289,78 @@ def batch_cpu_baseline(specs, nnz, iterations, sample: int = 8):
     iteration per nonzero from them, times each instance's nonzeros and the
     iterations its device solve took, summed over the instances and shared
     over the cores."""
-    import multiprocessing as mp
     cores = os.cpu_count() or 1
     order = sorted(range(len(specs)), key=lambda i: nnz[i])
     picks = sorted({order[round(k * (len(order) - 1) / max(1, sample - 1))] for k in range(min(sample, len(order)))})
-    with mp.get_context("spawn").Pool(min(cores, len(picks))) as pool:
-        per_iter = pool.map(_oracle_seconds_per_iteration, [specs[i] for i in picks])
+    per_iter = pool.map(_oracle_seconds_per_iteration, [specs[i] for i in picks])
     rate = float(np.median([t / nnz[i] for t, i in zip(per_iter, picks)]))
     cpu_seconds = sum(rate * nnz[i] * iterations[i] for i in range(len(specs))) / cores
-    return {"value": len(specs) / cpu_seconds, "unit": "LPs/s", "cores": cores, "kind": "port",
-            "sample": f"{len(picks)} of the instances timed over 16 FP64 PDHG iterations each on the oracle, one "
-                      f"process per instance; {rate * 1e9:.2f} ns per nonzero-iteration extrapolated to every "
-                      f"instance's nonzeros and the iterations its device solve took, over {cores} cores"}
+    return {"value": len(specs) / cpu_seconds, "unit": "LPs/s", "cores": cores, "kind": "port", "extrapolated": True,
+            "sample": f"ESTIMATED: {len(picks)} of the instances timed over 16 FP64 PDHG iterations each on the "
+                      f"oracle, one process per instance; {rate * 1e9:.2f} ns per nonzero-iteration extrapolated to "
+                      f"every instance's nonzeros and the iterations its device solve took, over {cores} cores"}
 
 
-def run_batch(args, rank, world, dist, barrier):
+def run_batch(args, rank, world, dist, pool):
     """Config 3: an uneven sweep of ``--batch`` DC-LOPF instances (buses
     U{100..2000}, snapshots U{24..168}, load scale U[0.6, 0.95], seeded), FP32
     refinement to 1e-6, each pass one launch for all of this rank's
-    instances.  Ranks take longest-processing-time shards; LPs/s is all
-    instances over the slowest rank's time."""
+    instances (host buffers in and out: upload, equilibration and download
+    are inside the wall time).  Ranks take longest-processing-time shards;
+    LPs/s is all instances over the slowest rank's device span."""
     import torch
     from noaidi_b200.prima import MixedPrecisionParams, PdhgParams, cuda, generators as G
     from noaidi_b200.prima.sharding import instance_size, shard
     problems = G.lopf_batch(seed=0, count=args.batch)
+    specs = _batch_specs(0, args.batch)
     mine = shard([instance_size(p) for p in problems], world)[rank]
     params = PdhgParams(eps_abs=BATCH_EPS, eps_rel=BATCH_EPS, max_iterations=args.max_iterations)
     mixed = MixedPrecisionParams(reduced_max_iterations=args.max_iterations)
     ctx = cuda.Context(int(os.environ.get("LOCAL_RANK", "0")), 32)
-    barrier()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t = time.perf_counter()
     res = cuda.mixed_solve_batch([problems[i] for i in mine], params, mixed, scheme=cuda.MIXED_REFINEMENT,
                                  round_reduction=args.round_reduction, ctx=ctx) if mine else []
     torch.cuda.synchronize()
     secs = time.perf_counter() - t
     span = max((r.solution.span_ms for r in res), default=0.0) / 1e3
+    kern = max((r.solution.device_ms for r in res), default=0.0) / 1e3
     agg = torch.tensor([span, secs], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(agg, op=dist.ReduceOp.MAX)
     ctx.close()
     its = [r.reduced_iterations + r.refinement_iterations for r in res]
     statuses = sorted({r.solution.status.name for r in res})
-    cpu = None
-    if rank == 0 and res and not args.skip_cpu:
-        specs = _batch_specs(0, args.batch)
-        cpu = batch_cpu_baseline([specs[i] for i in mine], [problems[i].constraint_matrix.nnz for i in mine], its)
-    return {"workload": f"config 3: {args.batch} uneven DC-LOPF instances, FP32 refinement to {BATCH_EPS:g}",
-            "cpu_baseline": cpu,
-            "instances": args.batch, "lps_per_s": args.batch / float(agg[0]), "seconds": float(agg[0]),
-            "wall_seconds": float(agg[1]), "statuses_rank0": statuses,
-            "iterations_rank0": {"min": int(min(its)), "median": float(np.median(its)), "max": int(max(its))}
-            if its else None,
-            "columns": int(sum(p.num_variables for p in problems)),
-            "nnz": int(sum(p.constraint_matrix.nnz for p in problems))}
+    out = {"workload": f"config 3: {args.batch} uneven DC-LOPF instances (buses U{{100..2000}}, snapshots "
+                       f"U{{24..168}}), FP32 refinement to {BATCH_EPS:g}",
+           "instances": args.batch, "lps_per_s": args.batch / float(agg[0]), "seconds": float(agg[0]),
+           "wall_seconds": float(agg[1]), "statuses_rank0": statuses,
+           "iterations_rank0": {"min": int(min(its)), "median": float(np.median(its)), "max": int(max(its))}
+           if its else None,
+           "columns": int(sum(p.num_variables for p in problems)),
+           "nnz": int(sum(p.constraint_matrix.nnz for p in problems))}
+    if rank == 0 and res:
+        pk, pk_src = peaks()
+        byts = sum(algorithmic_bytes(problems[i], r.solution.trials, r.reduced_iterations + r.refinement_iterations,
+                                     4, anchored=True) for i, r in zip(mine, res))
+        achieved = byts / max(kern, 1e-9) / 1e9 if kern > 0 else None
+        out["roofline"] = {"kernel": "pdhg_batch_kernel<float>", "bound": "hbm", "achieved": achieved,
+                           "peak": pk["hbm_gbs"], "unit": "GB/s",
+                           "frac": achieved / pk["hbm_gbs"] if achieved else None, "peak_source": pk_src,
+                           "note": "algorithmic bytes of every instance's trials over the longest pass sum of device "
+                                   "time (the launches of one pass run concurrently)"}
+        # errors against HiGHS on the three smallest instances of this rank
+        small = sorted(range(len(mine)), key=lambda k: instance_size(problems[mine[k]]))[:3]
+        highs = pool.map(_highs_lopf, [specs[mine[k]] for k in small]) if pool else []
+        errs = [rel_err(res[k].solution.objective_value, h) for k, h in zip(small, highs)]
+        out["error_vs_highs"] = {"instances": [int(mine[k]) for k in small],
+                                 "objective_rel_err_max": max(errs) if errs else None}
+        if not args.skip_cpu:
+            out["cpu_baseline"] = batch_cpu_baseline(pool, [specs[i] for i in mine],
+                                                     [problems[i].constraint_matrix.nnz for i in mine], its)
+    return out
 
 
 def profile_problem(workload: str, snapshots: int):
@@ -299,9 +403,40 @@ def run_profile_case(args) -> None:
         s = resident.solve(params, want_solution=False)
         out.update(precision=args.profile_precision)
     out.update(status=s.status.name, objective=s.objective_value, iterations=s.iterations, trials=s.trials,
-               device_s=s.device_ms / 1e3, us_per_trial=1e3 * s.device_ms / max(1, s.trials))
+               blocks=s.blocks, device_s=s.device_ms / 1e3, us_per_trial=1e3 * s.device_ms / max(1, s.trials))
     resident.free()
     print(json.dumps(out), flush=True)
+
+
+def run_fp64_study(args) -> None:
+    """The FP32 refinement against plain FP64 device PDHG, both solved to
+    --eps in full, on every seed of --fp64-study: times, iterations, statuses,
+    objectives and the speed-up per seed and its median (one JSON line)."""
+    from noaidi_b200.prima import MixedPrecisionParams, PdhgParams, cuda, generators as G
+    seeds = [int(s) for s in args.fp64_study.split(",")]
+    params = PdhgParams(eps_abs=args.eps, eps_rel=args.eps, max_iterations=args.max_iterations)
+    mixed = MixedPrecisionParams(reduced_max_iterations=args.max_iterations)
+    rows = []
+    for seed in seeds:
+        p = G.dc_lopf(seed=seed, **WORKLOAD)
+        r32 = cuda.DeviceProblem(p, params, ctx=cuda.Context(0, 32))
+        r = r32.mixed_solve(params, mixed, scheme=cuda.MIXED_REFINEMENT, round_reduction=args.round_reduction,
+                            want_solution=False)
+        r32.free()
+        r64 = cuda.DeviceProblem(p, params, ctx=cuda.Context(0, 64))
+        f = r64.solve(params, want_solution=False)
+        r64.free()
+        h = highs_reference(seed, p)
+        rows.append({"seed": seed, "refinement_s": r.solution.span_ms / 1e3, "fp64_s": f.span_ms / 1e3,
+                     "speedup": f.span_ms / r.solution.span_ms, "refinement_iterations":
+                     [r.reduced_iterations, r.refinement_iterations], "fp64_iterations": f.iterations,
+                     "status": [r.solution.status.name, f.status.name],
+                     "objective": [r.solution.objective_value, f.objective_value],
+                     "rel_err_vs_fp64": rel_err(r.solution.objective_value, f.objective_value),
+                     "rel_err_vs_highs": [rel_err(r.solution.objective_value, h), rel_err(f.objective_value, h)]})
+        print(json.dumps(rows[-1]), flush=True)
+    print(json.dumps({"fp64_study": rows, "eps": args.eps,
+                      "median_speedup": float(np.median([r["speedup"] for r in rows]))}), flush=True)
 
 
 def main():
@@ -311,18 +446,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--max-iterations", type=int, default=5_000_000)
-    ap.add_argument("--eps", type=float, default=EPS,
-                    help="relative KKT tolerance of the timed solves; at any value but 1e-8 the FP64 comparison "
-                         "arm is solved in full rather than sampled")
+    ap.add_argument("--eps", type=float, default=EPS, help="relative KKT tolerance of the timed solves")
     ap.add_argument("--round-reduction", type=float, default=ROUND_REDUCTION)
-    ap.add_argument("--fp64-sample-iterations", type=int, default=20_000)
-    ap.add_argument("--fp64-iterations", type=int, default=2_000_000)
-    ap.add_argument("--full-fp64", action="store_true", help="solve FP64 to tolerance instead of sampling")
+    ap.add_argument("--e2e-steps", type=int, default=3,
+                    help="one-shot solves with host buffers for the e2e figure (at most --steps)")
+    ap.add_argument("--skip-fp64", action="store_true", help="leave out the full FP64 comparison solve")
     ap.add_argument("--cpu-sample-iterations", type=int, default=128)
     ap.add_argument("--skip-cpu", action="store_true")
-    ap.add_argument("--batch", type=int, default=0,
-                    help="also solve this many config-3 instances (uneven LOPF sweep) to 1e-6 as batches "
-                         "and report LPs/s under 'batch' (0: off)")
+    ap.add_argument("--batch", type=int, default=256,
+                    help="config 3: solve this many uneven LOPF instances to 1e-6 as batches and report LPs/s under "
+                         "'batch' (0: off)")
+    ap.add_argument("--fp64-study", default="",
+                    help="comma-separated seeds: only compare the refinement with plain FP64, both in full, per seed")
     ap.add_argument("--profile-iterations", type=int, default=0,
                     help="only run this many PDHG iterations of the workload (a bounded case for ncu) and exit")
     ap.add_argument("--profile-precision", type=int, default=32, choices=[32, 64])
@@ -335,11 +470,18 @@ def main():
         return run_reference(args)
     if args.profile_iterations:
         return run_profile_case(args)
+    if args.fp64_study:
+        return run_fp64_study(args)
+
+    import multiprocessing as mp
 
     import torch
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    # the CPU legs run in spawned processes (none inherits a GPU context),
+    # started before the first GPU call
+    pool = mp.get_context("spawn").Pool(max(1, min(8, os.cpu_count() or 1))) if rank == 0 else None
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -351,8 +493,6 @@ def main():
 
     problem = G.dc_lopf(seed=rank, **WORKLOAD)
     eps = args.eps
-    if eps != EPS:  # the recorded FP64 iteration count is for 1e-8: measure the FP64 solve in full instead
-        args.full_fp64 = True
     params = PdhgParams(eps_abs=eps, eps_rel=eps, max_iterations=args.max_iterations)
     mixed = MixedPrecisionParams(reduced_max_iterations=args.max_iterations)
     ctx32 = cuda.Context(local, 32)
@@ -378,10 +518,15 @@ def main():
     span_s = sum(r.solution.span_ms for r in results) / 1e3
     kern_s = sum(r.solution.device_ms for r in results) / 1e3
 
+    # CPU legs on the host cores while the device runs the comparison solves
+    cpu_jobs = {}
+    if pool is not None and not args.skip_cpu:
+        cpu_jobs["config1"] = pool.apply_async(config1_oracle)
+
     # end to end through the one-shot C ABI call with host buffers
     barrier()
-    e2e = []
-    for _ in range(args.steps):
+    e2e, e2e_steps = [], max(1, min(args.e2e_steps, args.steps))
+    for _ in range(e2e_steps):
         t = time.perf_counter()
         r_e2e = cuda.mixed_solve(problem, params, mixed, scheme=cuda.MIXED_REFINEMENT,
                                  round_reduction=args.round_reduction, ctx=ctx32)
@@ -393,14 +538,25 @@ def main():
         dist.all_reduce(agg, op=dist.ReduceOp.MAX)
     max_span, max_e2e = float(agg[0]), float(agg[1])
 
-    # plain FP64 device PDHG on the same resident problem
-    ctx64 = cuda.Context(local, 64)
-    res64 = cuda.DeviceProblem(problem, params, ctx=ctx64)
-    p64 = params if args.full_fp64 else params.copy(max_iterations=args.fp64_sample_iterations)
-    fp64 = res64.solve(p64, want_solution=False)
-    fp64_ms_per_iter = fp64.device_ms / max(1, fp64.iterations)
+    # plain FP64 device PDHG on the same instance, solved in full
+    fp64 = None
+    if not args.skip_fp64:
+        ctx64 = cuda.Context(local, 64)
+        res64 = cuda.DeviceProblem(problem, params, ctx=ctx64)
+        fp64 = res64.solve(params, want_solution=False)
+        res64.free()
+        ctx64.close()
 
-    batch_line = run_batch(args, rank, world, dist, barrier) if args.batch else None
+    # config 1 on the device: the 600-column LP to 1e-6, one-shot calls
+    c1p = config1_problem()
+    c1params = PdhgParams(eps_abs=CONFIG1_EPS, eps_rel=CONFIG1_EPS, max_iterations=1_000_000)
+    cuda.mixed_solve(c1p, c1params, ctx=ctx32)  # warm
+    t = time.perf_counter()
+    c1_dev = cuda.mixed_solve(c1p, c1params, scheme=cuda.MIXED_REFINEMENT, ctx=ctx32)
+    c1_dev_s = time.perf_counter() - t
+    c1_64 = cuda.solve(c1p, c1params, precision=64)
+
+    batch_line = run_batch(args, rank, world, dist, pool) if args.batch else None
 
     if rank == 0:
         pk, pk_src = peaks()
@@ -413,12 +569,9 @@ def main():
             "unit": UNIT, "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * max_span / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 iterate, f64 anchor/KKT", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "n": n, "m": m, "nnz": nnz, "eps": eps, "seed": "rank",
-                       "parallelism": f"independent instances x{world}", "scheme": "fp32 pass + fp32 refinement "
-                       f"around an fp64 anchor, round reduction {args.round_reduction:g}",
-                       "l2": "working set larger than L2 (no flush needed)"},
+            "config": bench_config(problem, eps, world, args.round_reduction),
             "clocks": clocks.summary(),
-            "e2e": {"value": steps * world / max_e2e, "unit": UNIT,
+            "e2e": {"value": e2e_steps * world / max_e2e, "unit": UNIT, "steps": e2e_steps,
                     "h2d_bytes_per_step": int(nnz * 12 + (m + 1) * 4 + 8 * (3 * n + m)),
                     "d2h_bytes_per_step": int(8 * (2 * n + m))},
             "gpu_launches": 2 * steps,
@@ -427,16 +580,23 @@ def main():
                          "dual_residual": sol.kkt.dual_residual_norm, "gap": sol.kkt.absolute_gap,
                          "fp32_pass_iterations": last.reduced_iterations,
                          "refinement_iterations": last.refinement_iterations,
-                         "rounds": last.refinement_rounds, "e2e_status": r_e2e.solution.status.name},
+                         "rounds": last.refinement_rounds, "blocks": sol.blocks,
+                         "e2e_status": r_e2e.solution.status.name},
         }
-        iters64 = fp64.iterations if args.full_fp64 and fp64.status.name == "OPTIMAL" else \
-            (FP64_ITERATIONS_TO_TOLERANCE or args.fp64_iterations)
-        fp64_ttt = fp64_ms_per_iter * iters64
-        line["fp64_baseline"] = {
-            "ms_per_iteration": fp64_ms_per_iter, "iterations_to_tolerance": iters64,
-            "time_to_tolerance_ms": fp64_ttt, "measured": "full solve" if args.full_fp64 else
-            f"{fp64.iterations}-iteration sample x iterations of a full FP64 solve", "status": fp64.status.name,
-            "speedup_of_fp32_refinement": fp64_ttt / (1e3 * max_span / steps)}
+        h = highs_reference(0, problem) if rank == 0 else None
+        line["error"] = {"objective_rel_err_vs_highs": rel_err(sol.objective_value, h), "highs_objective": h}
+        iters64 = FP64_ITERATIONS_TO_TOLERANCE
+        if fp64 is not None:
+            iters64 = fp64.iterations
+            fp64_s = fp64.span_ms / 1e3
+            line["fp64_baseline"] = {
+                "measured": "full solve to tolerance, once per run", "time_to_tolerance_ms": 1e3 * fp64_s,
+                "device_ms": fp64.device_ms, "iterations_to_tolerance": fp64.iterations,
+                "ms_per_iteration": fp64.device_ms / max(1, fp64.iterations), "status": fp64.status.name,
+                "objective": fp64.objective_value, "status_identical": fp64.status == sol.status,
+                "speedup_of_fp32_refinement": fp64_s / (max_span / steps)}
+            line["error"]["objective_rel_err_vs_fp64"] = rel_err(sol.objective_value, fp64.objective_value)
+            line["error"]["fp64_objective_rel_err_vs_highs"] = rel_err(fp64.objective_value, h)
         trials32 = sum(r.solution.trials for r in results)
         iters32 = sum(r.reduced_iterations + r.refinement_iterations for r in results)
         byts = algorithmic_bytes(problem, trials32, iters32, 4, anchored=True)
@@ -446,26 +606,31 @@ def main():
                             "traffic": TRAFFIC_BYTES_PER_TRIAL * trials32 / len(results) if TRAFFIC_BYTES_PER_TRIAL else None,
                             "peak_source": pk_src,
                             "per_trial_bytes": byts / max(1, trials32), "kernel_ms": 1e3 * kern_s / steps}
+        c1 = cpu_jobs["config1"].get() if "config1" in cpu_jobs else None
+        line["config1"] = {"workload": "random sparse LP m=400 n=600 (5 nonzeros per column), seed 0",
+                           "eps": CONFIG1_EPS, "device_refinement_s": c1_dev_s,
+                           "device_status": c1_dev.solution.status.name,
+                           "device_iterations": [c1_dev.reduced_iterations, c1_dev.refinement_iterations],
+                           "device_fp64_s": c1_64.solve_time_millis / 1e3, "device_fp64_iterations": c1_64.iterations,
+                           "oracle": c1, "measured": "every figure a full solve to tolerance"}
         if batch_line:
             line["batch"] = batch_line
         if not args.skip_cpu:
             per_iter, done = cpu_sample(problem, args.cpu_sample_iterations)
             lps = 1.0 / (per_iter * iters64)
-            line["cpu_baseline"] = {"value": lps, "unit": UNIT, "cores": 1, "kind": "port",
-                                    "sample": f"{done} FP64 PDHG iterations of the same instance on one host core "
-                                              f"(oracle restatement of the reference), {per_iter * 1e3:.1f} "
-                                              f"ms/iteration extrapolated to {iters64} iterations"}
+            line["cpu_baseline"] = {"value": lps, "unit": UNIT, "cores": 1, **host_info(), "kind": "port",
+                                    "extrapolated": True,
+                                    "sample": f"EXTRAPOLATED, not solved: {done} FP64 PDHG iterations of the same "
+                                              f"instance on one host core (the oracle, the reference's FP64 PDHG "
+                                              f"restated), {per_iter * 1e3:.1f} ms/iteration, times the {iters64} "
+                                              f"iterations the FP64 device solve of this run needed"}
         print(json.dumps(line), flush=True)
     ctx32.close()
-    ctx64.close()
+    if pool is not None:
+        pool.close()
     if dist:
         dist.destroy_process_group()
 
-
-# DRAM bytes (read + write) per step-size trial of pdhg_kernel<float> on this
-# workload, from an ncu capture of a bounded run of the same instance; None
-# until measured.
-TRAFFIC_BYTES_PER_TRIAL = 140.5e6
 
 if __name__ == "__main__":
     main()

@@ -68,6 +68,16 @@ int32_t prima_open(int32_t device, int32_t precision_bits, prima_handle *ctx);
  * context.  Idempotent: closing a closed context returns PRIMA_OK. */
 int32_t prima_close(prima_handle ctx);
 int32_t prima_capabilities_get(prima_handle ctx, prima_capabilities *out);
+/* The number of polls a block of the persistent solver makes while waiting
+ * at a team barrier for the other blocks before it gives up, raises the
+ * team's abort flag and the call returns PRIMA_ERR_TIMEOUT (the reference's
+ * solve loop has no such wait: Pdhg.scala:206-246 runs on one thread).
+ * polls = 0 restores the default, 2^26 polls (seconds; a phase takes
+ * microseconds).  A small value makes every multi-block solve of this context
+ * give up at once, which is how the timeout path is exercised; the waits for
+ * a block's own bulk copies keep their fixed bound.  No counterpart in the
+ * reference. */
+int32_t prima_set_device_wait_limit(prima_handle ctx, int64_t polls);
 
 /* ---- memory (Kernels.scala:51-63) ---------------------------------------- */
 /* Kernels.allocate: a zero-filled vector of length n. */
@@ -106,8 +116,13 @@ int32_t prima_squared_norm(prima_handle ctx, prima_handle x, double *out);
  * larger n is rejected with PRIMA_ERR_INVALID_ARGUMENT.  The block partials
  * live in a fixed 16 KiB device array that every GPU loading the library
  * holds until exit; the first call on each device looks up its address and
- * should come before any stream capture.  Calls that overlap on the GPU race
- * on that array. */
+ * should come before any stream capture.  The address is cached per CUDA
+ * context: a device reset (cudaDeviceReset, a primary-context reset) moves
+ * the array, and the first call after it looks the address up again.  x, y
+ * and out are checked to be memory of the current device (or managed) before
+ * anything is queued; a host pointer or another GPU's memory is refused with
+ * PRIMA_ERR_INVALID_ARGUMENT.  Calls that overlap on the GPU race on that
+ * array. */
 int32_t prima_dot_no_alloc(const void *x, const void *y, int64_t n, int32_t element_bits, double *out,
                            void *stream);
 /* out := clamp(x - tau*(cost - kty), lower, upper), two-comparison clamp */
@@ -182,6 +197,8 @@ typedef struct {
   double setup_ms;  /* scaling, transpose and upload */
   int64_t trials;   /* step-size trials, accepted and rejected */
   double span_ms;   /* CUDA-event time from the call's first device work to its last */
+  int32_t blocks;   /* blocks of the persistent kernel's team that ran the (last) pass */
+  int32_t pad2;
 } prima_solution_info;
 
 /* Pdhg.solveWith(problem, params, this-context, cancelled, warmStart).
@@ -268,6 +285,14 @@ int32_t prima_problem_free(prima_handle ctx, prima_handle problem);
  * (BranchAndBound.scala:264-276, the node's LpProblem with new
  * variableLower/variableUpper). */
 int32_t prima_problem_set_bounds(prima_handle ctx, prima_handle problem, const double *lower, const double *upper);
+/* Scaling.apply's result for the resident problem (Scaling.scala:77-155), as
+ * the device computed it: the equilibrated matrix values in the caller's CSR
+ * order (nnz), the equilibrated objective, bounds (n) and right-hand side (m),
+ * and the cumulative row and column scales that undo it.  Any output may be
+ * NULL.  No counterpart in the reference (its ScaledProblem is a host
+ * object); offered so a caller can inspect or verify the scaling. */
+int32_t prima_problem_scaled(prima_handle ctx, prima_handle problem, double *values, double *objective,
+                             double *rhs, double *lower, double *upper, double *row_scale, double *col_scale);
 /* As prima_pdhg_solve / prima_mixed_solve on a resident problem. */
 int32_t prima_problem_solve(prima_handle ctx, prima_handle problem, const prima_params *params,
                             const prima_warm_start *warm_start, const volatile int32_t *cancel,

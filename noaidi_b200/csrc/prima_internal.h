@@ -139,6 +139,7 @@ struct Ctx {
   double *host_scalar = nullptr;  // pinned: reduction results
   int32_t *cancel_mapped = nullptr;  // pinned + mapped: cancel flag seen by the device
   int32_t *cancel_mapped_dev = nullptr;
+  int64_t wait_limit = 0;      // team-barrier polls before a block gives up (0: the default)
   DeviceBuffer solver_arena;   // buffers of the coarse solvers, reused across solves
   DeviceBuffer batch_arena;    // state, arguments and queue of a batch launch
   PreparedLp scratch_lp;       // the problem of a one-shot solve call

@@ -12,10 +12,18 @@
 // library holds until the process exits.  Host code cannot use the array's
 // name as a device address, so the first call on each device (with that
 // device current) looks up the array's device address with
-// cudaGetSymbolAddress and caches it; that first call should come before any
-// stream capture.  All calls on a device share the array: calls whose
-// kernels overlap on the GPU (two streams, two threads) race on it.  Nothing
-// in it has to start at zero: a call writes every partial it reads.
+// cudaGetSymbolAddress and caches it, keyed by the current CUDA context's
+// ID; that first call should come before any stream capture.  A reset of the
+// device (cudaDeviceReset, or a reset of the primary context) loads the
+// module again at a new address: the next call sees the new context ID and
+// looks the address up again.  All calls on a device share the array: calls
+// whose kernels overlap on the GPU (two streams, two threads) race on it.
+// Nothing in it has to start at zero: a call writes every partial it reads.
+//
+// The arrays come from the caller, so each pointer is checked to be memory
+// of the current device (cudaPointerGetAttributes, which allocates nothing)
+// before any kernel is queued; a host pointer or another GPU's memory is
+// refused, not read.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -74,26 +82,72 @@ __global__ void __launch_bounds__(kDotThreads) k_dot_total(const double *__restr
 }
 
 std::mutex g_setup_mu;
-double *g_partials_ptr[kMaxDevices] = {};
+struct PartialsAddress {
+  unsigned long long ctx_id = 0;  // the context the address belongs to
+  double *ptr = nullptr;
+};
+PartialsAddress g_partials[kMaxDevices];
 
-// The device address of g_dot_partials on the current device, looked up on
-// the first call per device.
-int32_t partials_on_current_device(double **out) {
-  int dev = -1;
-  PRIMA_CUDA_TRY(cudaGetDevice(&dev));
+// The ID of the calling thread's current CUDA context, through the driver
+// entry points the runtime hands out (the library does not link libcuda).
+typedef int (*CtxGetCurrentFn)(void **ctx);
+typedef int (*CtxGetIdFn)(void *ctx, unsigned long long *id);
+int32_t current_context_id(unsigned long long *id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void *f0 = nullptr, *f1 = nullptr;
+    cudaDriverEntryPointQueryResult q0, q1;
+    PRIMA_CUDA_TRY(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0));
+    PRIMA_CUDA_TRY(cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1));
+    if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1) {
+      set_error("prima_dot_no_alloc: the driver offers no cuCtxGetCurrent/cuCtxGetId");
+      return PRIMA_ERR_CUDA;
+    }
+    get_current = (CtxGetCurrentFn)f0;
+    get_id = (CtxGetIdFn)f1;
+  }
+  void *ctx = nullptr;
+  if (get_current(&ctx) != 0 || !ctx || get_id(ctx, id) != 0) {
+    set_error("prima_dot_no_alloc: no current CUDA context on this thread");
+    return PRIMA_ERR_CUDA;
+  }
+  return PRIMA_OK;
+}
+
+// The device address of g_dot_partials in the current context, looked up on
+// the first call per device and again whenever the device's context changed.
+int32_t partials_on_current_device(int dev, double **out) {
   if (dev < 0 || dev >= kMaxDevices) {
     set_error("prima_dot_no_alloc: device ordinal " + std::to_string(dev) + " is beyond the supported " +
               std::to_string(kMaxDevices));
     return PRIMA_ERR_INVALID_ARGUMENT;
   }
   std::lock_guard<std::mutex> lock(g_setup_mu);
-  if (!g_partials_ptr[dev]) {
+  unsigned long long id = 0;
+  int32_t rc = current_context_id(&id);
+  if (rc) return rc;
+  if (!g_partials[dev].ptr || g_partials[dev].ctx_id != id) {
     void *ptr = nullptr;
     PRIMA_CUDA_TRY(cudaGetSymbolAddress(&ptr, g_dot_partials));
-    g_partials_ptr[dev] = (double *)ptr;
+    g_partials[dev].ptr = (double *)ptr;
+    g_partials[dev].ctx_id = id;
   }
-  *out = g_partials_ptr[dev];
+  *out = g_partials[dev].ptr;
   return PRIMA_OK;
+}
+
+// True when p is memory the current device's kernels may read or write:
+// device memory of that device, or managed memory.
+bool on_device(const void *p, int dev) {
+  cudaPointerAttributes attr;
+  const cudaError_t e = cudaPointerGetAttributes(&attr, p);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();  // an unrecognised pointer: refused, not the caller's pending error
+    return false;
+  }
+  if (attr.type == cudaMemoryTypeManaged) return true;
+  return attr.type == cudaMemoryTypeDevice && attr.device == dev;
 }
 
 }  // namespace
@@ -124,20 +178,28 @@ extern "C" int32_t prima_dot_no_alloc(const void *x, const void *y, int64_t n, i
     set_error("prima_dot_no_alloc: x and y must be aligned to their element size and out to 8 bytes");
     return PRIMA_ERR_INVALID_ARGUMENT;
   }
+  int dev = -1;
+  PRIMA_CUDA_TRY(cudaGetDevice(&dev));
+  if (!on_device(out, dev) || (n > 0 && (!on_device(x, dev) || !on_device(y, dev)))) {
+    set_error("prima_dot_no_alloc: x, y and out must be memory of the current device (device " + std::to_string(dev) +
+              ") or managed memory; a host pointer or another GPU's memory is refused");
+    return PRIMA_ERR_INVALID_ARGUMENT;
+  }
   double *partials = nullptr;
-  int32_t rc = partials_on_current_device(&partials);
+  int32_t rc = partials_on_current_device(dev, &partials);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   if (n == 0) {
     PRIMA_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double), s));
     return PRIMA_OK;
   }
-  const int nb = (int)((n + kDotSpan - 1) / kDotSpan);
-  if (element_bits == 64)
-    k_dot_span<double><<<nb, kDotThreads, 0, s>>>((const double *)x, (const double *)y, n, partials);
-  else
-    k_dot_span<float><<<nb, kDotThreads, 0, s>>>((const float *)x, (const float *)y, n, partials);
-  k_dot_total<<<1, kDotThreads, 0, s>>>(partials, nb, out);
-  PRIMA_CUDA_TRY(cudaGetLastError());
+  // Each launch's own status is checked (not the thread's last-error slot,
+  // which may hold an error the caller left there earlier).
+  int nb = (int)((n + kDotSpan - 1) / kDotSpan);
+  void *span_args[] = {(void *)&x, (void *)&y, (void *)&n, (void *)&partials};
+  const void *span = element_bits == 64 ? (const void *)k_dot_span<double> : (const void *)k_dot_span<float>;
+  PRIMA_CUDA_TRY(cudaLaunchKernel(span, dim3(nb), dim3(kDotThreads), span_args, 0, s));
+  void *total_args[] = {(void *)&partials, (void *)&nb, (void *)&out};
+  PRIMA_CUDA_TRY(cudaLaunchKernel((const void *)k_dot_total, dim3(1), dim3(kDotThreads), total_args, 0, s));
   return PRIMA_OK;
 }

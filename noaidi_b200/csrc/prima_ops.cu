@@ -371,6 +371,19 @@ extern "C" int32_t prima_capabilities_get(prima_handle h, prima_capabilities *ou
   return PRIMA_OK;
 }
 
+extern "C" int32_t prima_set_device_wait_limit(prima_handle h, int64_t polls) {
+  clear_error();
+  int32_t rc;
+  Ctx *c = lookup_ctx(h, &rc);
+  if (!c) return rc;
+  if (polls < 0) {
+    set_error("requirement failed: the wait limit must be non-negative (0 restores the default)");
+    return PRIMA_ERR_INVALID_ARGUMENT;
+  }
+  c->wait_limit = polls;
+  return PRIMA_OK;
+}
+
 // ---- memory ---------------------------------------------------------------
 #define CTX_OR_RETURN(h)        \
   clear_error();                \

@@ -34,6 +34,25 @@ __device__ __forceinline__ unsigned atom_add_acq_rel(unsigned *p, unsigned v) {
   asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
   return old;
 }
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long atom_add_acq_rel_u64(unsigned long long *p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+#ifndef PRIMA_POLL_SLEEP_NS
+#define PRIMA_POLL_SLEEP_NS 32
+#endif
+#ifndef PRIMA_GROUP_RELEASE
+#define PRIMA_GROUP_RELEASE 0
+#endif
 __device__ __forceinline__ uint64_t global_timer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -177,12 +196,15 @@ __device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *b, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
 }
+// One poll of an mbarrier phase: the thread may be suspended until the phase
+// completes, but for no more than kSuspendNs.
+constexpr unsigned kSuspendNs = 10000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *b, unsigned parity) {
   unsigned ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
       : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
+      : "r"(smem_u32(b)), "r"(parity), "r"(kSuspendNs)
       : "memory");
   return ok != 0;
 }
@@ -195,14 +217,52 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned b
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
-constexpr long long kMbarSpinLimit = 1ll << 24;  // try_wait polls; each may suspend briefly
+// A stage's bytes land within microseconds; a wait that has lasted this long
+// has failed.
+constexpr unsigned long long kStageWaitNs = 2000000000ull;
 
-// Bounded wait for a buffer's bulk copies.  False: gave up (the caller
-// raises the team's abort flag and leaves).
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity) {
-  for (long long i = 0; i < kMbarSpinLimit; i++)
+__device__ __forceinline__ uint64_t stage_timer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for a buffer's bulk copies, by the clock (a poll may suspend
+// the thread, so counting polls would bound nothing).  False: gave up, or
+// the team's abort flag went up (when given); the caller raises the team's
+// abort flag and leaves.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity, const int32_t *abort_flag = nullptr) {
+  if (mbar_try_wait(b, parity)) return true;
+  const uint64_t t0 = stage_timer_ns();
+  for (unsigned i = 1;; i++) {
     if (mbar_try_wait(b, parity)) return true;
-  return false;
+    if ((i & 15) == 0) {
+      if (abort_flag && *((const volatile int32_t *)abort_flag)) return false;
+      if (stage_timer_ns() - t0 > kStageWaitNs) return false;
+    }
+  }
+}
+
+// A word of the block's progress record (PRIMA_DEBUG_PROGRESS), if any.
+__device__ __forceinline__ void progress(volatile int32_t *rec, int word, int32_t v) {
+  if (rec && blockIdx.x < 256) rec[blockIdx.x * 16 + word] = v;
+}
+
+// Where a stage wait gave up, for the error the host reports: the first
+// failure of a launch fills diag[0..7] = {1, tag (1: phase A, 2: phase B),
+// 0, stage, parity, tile of the batch, tiles of this block, block}.
+__device__ __forceinline__ void note_stage_failure(int32_t *diag, int tag, int stage, unsigned parity, int j,
+                                                   int mine, int block) {
+  if (diag && atomicCAS(diag, 0, 1) == 0) {
+    diag[1] = tag;
+    diag[2] = 0;
+    diag[3] = stage;
+    diag[4] = (int32_t)parity;
+    diag[5] = j;
+    diag[6] = mine;
+    diag[7] = block;
+    __threadfence();
+  }
 }
 
 struct HotShared {
@@ -213,6 +273,9 @@ struct HotShared {
   int flag;
   int primed;                      // the next hot phase's first stages are already issued
   const int2 *listed;              // the table whose first batch hs.tiles holds, else nullptr
+  int tag;                         // unused slot kept for the failure record's layout
+  int32_t *diag;                   // the launch's failure record, or nullptr
+  volatile int32_t *prog;          // the launch's progress record, or nullptr
 };
 
 // The tile engine over a table of ntiles tiles (see above).  rp == nullptr:
@@ -303,7 +366,7 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
                                           const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
                                           const T *__restrict__ v, const T *xg, const T *const *vecs, int nv,
                                           unsigned char *smem, HotShared &hs, unsigned &par, int32_t *abort_flag,
-                                          Epi &&epi) {
+                                          int tag, Epi &&epi) {
   using L = HotLayout<T>;
   constexpr int S = L::kStages;
   const bool spmv = rp != nullptr;
@@ -338,8 +401,12 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
     int j = 0;
     for (; j < nj; j++) {
       const int b = j % S;
-      if (!__all_sync(0xffffffffu, mbar_wait(&hs.bars[b], (par >> b) & 1u))) {
-        if (lane == 0) atomicExch(abort_flag, 1);
+      if (!__all_sync(0xffffffffu, mbar_wait(&hs.bars[b], (par >> b) & 1u, abort_flag))) {
+        if (lane == 0) {
+          if (!*((const volatile int32_t *)abort_flag))
+            note_stage_failure(hs.diag, tag, b, (par >> b) & 1u, jb + j, mine, (int)blockIdx.x);
+          atomicExch(abort_flag, 1);
+        }
         break;
       }
       par ^= 1u << b;
@@ -497,10 +564,11 @@ __device__ __forceinline__ double (&reduction_scratch())[kMaxQ][kWarps] {
 
 // Block-wide totals of Q per-thread values in a fixed order.  The block's
 // totals go to shared s_part[base..base+Q) and, in a multi-block team, to the
-// global partials[(base + q) * stride + rank].
+// global partials[(gbase + q) * stride + rank] (gbase = base unless given).
 template <int Q>
 __device__ __forceinline__ void block_partials(const double (&v)[Q], double *partials, int stride, int rank, int nb,
-                                               int base, double *s_part) {
+                                               int base, double *s_part, int gbase = -1) {
+  if (gbase < 0) gbase = base;
   double(&sh)[kMaxQ][kWarps] = reduction_scratch();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -516,21 +584,22 @@ __device__ __forceinline__ void block_partials(const double (&v)[Q], double *par
 #pragma unroll
     for (int w = 0; w < kWarps; w++) s += sh[threadIdx.x][w];
     s_part[base + threadIdx.x] = s;
-    if (nb > 1) partials[(base + threadIdx.x) * stride + rank] = s;
+    if (nb > 1) partials[(gbase + threadIdx.x) * stride + rank] = s;
   }
   __syncthreads();
 }
 
-// Deciding block: totals of slots [0, Q) over the nb block partials, in a
-// fixed order (the block's own shared totals when nb == 1).
+// Totals of slots [0, Q) over the nb block partials, in a fixed order (the
+// block's own shared totals when nb == 1); global slots start at gbase.
 template <int Q>
 __device__ __forceinline__ void reduce_partials(const double *partials, int stride, int nb, const double *s_part,
-                                                double *out) {
+                                                double *out, int gbase = 0) {
   if (nb == 1) {
     if (threadIdx.x < Q) out[threadIdx.x] = s_part[threadIdx.x];
     __syncthreads();
     return;
   }
+  partials += (int64_t)gbase * stride;
   double(&sh)[kMaxQ][kWarps] = reduction_scratch();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double v[Q];
@@ -878,7 +947,7 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
   if (s.pend) {
     const T *vecs[6] = {x, a.sx, a.skty, a.c, a.l, a.u};
     ok = hot_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], vecs, 6, smem, hs, par,
-                      &a.sync->abort, [&](int32_t j, int i, T kt, const T *sl) {
+                      &a.sync->abort, 1, [&](int32_t j, int i, T kt, const T *sl) {
                         constexpr int S = kHotRows<T>;
                         const T xj = sl[i], sx = sl[S + i], skt = sl[2 * S + i];
                         const T cj = sl[3 * S + i], lj = sl[4 * S + i], uj = sl[5 * S + i];
@@ -890,12 +959,12 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
   } else {
     const T *vecs[5] = {x, a.kty, a.c, a.l, a.u};
     ok = hot_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, nullptr, nullptr, nullptr, nullptr, vecs, 5, smem, hs, par,
-                      &a.sync->abort, [&](int32_t j, int i, T, const T *sl) {
+                      &a.sync->abort, 1, [&](int32_t j, int i, T, const T *sl) {
                         constexpr int S = kHotRows<T>;
                         step(j, sl[i], sl[S + i], sl[2 * S + i], sl[3 * S + i], sl[4 * S + i]);
                       });
   }
-  block_partials<1>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DX, tm.s_part);
+  block_partials<1>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DX, tm.s_part, hot_bank(s.total_trials) + Q_DX);
   return ok;
 }
 
@@ -930,7 +999,7 @@ __device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsi
   const int iylo = pend ? 5 : 3;
   const bool has_lo = a.ylo != nullptr;
   const bool ok = hot_tiles<T>(a.ntiles_k, tm.nb, tm.rank, a.tiles_k, a.kp, a.kci, a.kv, (const T *)a.xbar, vecs, nv, smem, hs, par,
-                               &a.sync->abort, [&](int32_t r, int i, T kb, const T *sl) {
+                               &a.sync->abort, 2, [&](int32_t r, int i, T kb, const T *sl) {
     constexpr int S = kHotRows<T>;
     const T yr = sl[i], kxr = sl[S + i], qr = sl[2 * S + i];
     const T syr = pend ? sl[3 * S + i] : T(0), skxr = pend ? sl[4 * S + i] : T(0);
@@ -949,7 +1018,7 @@ __device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsi
     v[0] += (double)dy * (double)dy;
     v[1] += (double)dy * (double)kdx;
   });
-  block_partials<2>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DY, tm.s_part);
+  block_partials<2>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DY, tm.s_part, hot_bank(s.total_trials) + Q_DY);
   return ok;
 }
 
@@ -1149,14 +1218,14 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
       // the step rule's two powers depend only on the iteration count: two
       // other warps evaluate them while the partials are being reduced
       __shared__ double s_pow[2];
-      const uint64_t t_in = (a.prof && threadIdx.x == 0) ? global_timer_ns() : 0;
+      const uint64_t t_in = (a.prof && threadIdx.x == 0 && tm.rank == 0) ? global_timer_ns() : 0;
       {
         const double t = (double)(c.iteration - c.period_base + 1);
         if (threadIdx.x == 32) s_pow[0] = pow(t, -0.3);
         if (threadIdx.x == 64) s_pow[1] = pow(t, -0.6);
       }
-      reduce_partials<3>(a.partials, a.max_blocks, tm.nb, tm.s_part, red);
-      if (a.prof && threadIdx.x == 0) a.prof->reduce_b_ns += global_timer_ns() - t_in;
+      reduce_partials<3>(a.partials, a.max_blocks, tm.nb, tm.s_part, red, hot_bank(c.total_trials));
+      if (a.prof && threadIdx.x == 0 && tm.rank == 0) a.prof->reduce_b_ns += global_timer_ns() - t_in;
       if (threadIdx.x == 0) {
         c.trials += 1;
         c.total_trials += 1;
@@ -1316,7 +1385,7 @@ __device__ void decide(const Args<T> &a, Control &c, int phase, const Team &tm, 
 
 // ---- the team barrier -------------------------------------------------------
 
-constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~seconds; a phase takes microseconds
+constexpr long long kDefaultSpinLimit = 1ll << 26;  // ~seconds; a phase takes microseconds
 
 // The team barrier's generation as this block last saw it.  Read from the
 // Sync record once when a solve starts -- no barrier of that solve can have
@@ -1326,6 +1395,20 @@ constexpr unsigned long long kSpinLimit = 1ull << 26;  // ~seconds; a phase take
 __device__ __forceinline__ unsigned &barrier_generation() {
   __shared__ unsigned s_gen;
   return s_gen;
+}
+
+// Hot barriers (after phases A and B) this block has passed in this solve:
+// the team's arrival counter reads nb times that when the last one released.
+__device__ __forceinline__ unsigned long long &hot_epoch() {
+  __shared__ unsigned long long s_ep;
+  return s_ep;
+}
+
+// Phase timing (PRIMA_PHASE_TIMES): when this block started its current hot
+// phase, and when it arrived at that phase's barrier.
+__device__ __forceinline__ uint64_t (&block_clock())[2] {
+  __shared__ uint64_t s_clock[2];
+  return s_clock;
 }
 
 template <typename T>
@@ -1364,6 +1447,7 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     const int nv = b_operands(a, snap, vecs);
     prime_tiles<T>(a.ntiles_k, tm.nb, tm.rank, a.tiles_k, a.kp, a.kci, a.kv, vecs, nv, smem, hs);
   };
+  auto list_a_tiles = [&] { list_tiles(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, hs); };
   __shared__ int s_last, s_ok;
   __shared__ double s_red[kMaxQ];
   if (tm.nb == 1) {
@@ -1394,12 +1478,140 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     __syncthreads();
     return true;
   }
+  if (phase == PH_A || phase == PH_B) {
+    // The trial's barriers.  Every block counts itself in on its group's
+    // arrival counter and the last of each group on the team's (neither is
+    // ever reset: the k-th barrier completes when the team's counter reads
+    // k * G), and waits for the whole team; after phase B every block then reduces the
+    // trial's partials itself, in the same fixed order, and takes the same
+    // step-size decision on its own copy of the Control record.  Nothing is
+    // published and no block waits for a deciding block: the decision inputs
+    // (partials, iteration counts, step, weight) are the same everywhere, and
+    // the decision reads no clock and no flag.
+    unsigned long long &s_ep = hot_epoch();
+    const int groups = tm.nb < kArriveGroups ? tm.nb : kArriveGroups;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned long long target = (s_ep + 1) * (unsigned long long)groups;
+      if (a.prof) {
+        const uint64_t now = global_timer_ns(), tr = ldv(&a.prof->t_release);
+        if (tr) {
+          const unsigned long long d = now - tr;
+          atomicAdd((unsigned long long *)&a.prof->arrive_ns[phase & 7], d);
+          if (tm.rank < kProfBlocks) {
+            a.prof->block_arrive[phase == PH_B][tm.rank] += d;  // this block's own slot
+            unsigned sm;
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+            a.prof->block_sm[tm.rank] = (int32_t)sm;
+            if (block_clock()[0]) a.prof->block_work[phase == PH_B][tm.rank] += now - block_clock()[0];
+          }
+        }
+        block_clock()[1] = now;
+      }
+      // count in on the group's counter; the group's last block counts the
+      // group in on the team's
+      const int g = tm.rank % groups;
+      const unsigned long long gsize = (unsigned long long)((tm.nb - g + groups - 1) / groups);
+      const unsigned long long gold = atom_add_acq_rel_u64(a.arrive_groups + (size_t)g * kArriveStride, 1ull);
+      s_last = 0;
+      if (gold + 1 == (s_ep + 1) * gsize) {
+        const unsigned long long old = atom_add_acq_rel_u64(&a.sync->arrive, 1ull);
+        s_last = old + 1 == target;
+      }
+      s_ok = 1;
+    }
+    __syncthreads();
+    if (prime && threadIdx.x >> 5 == 1) {
+      prime_b();
+    } else if (list_a && threadIdx.x >> 5 == 1) {
+      list_a_tiles();
+    } else if (threadIdx.x == 0) {
+      const unsigned long long target = (s_ep + 1) * (unsigned long long)groups;
+#if PRIMA_GROUP_RELEASE
+      // the team's last block writes every group's release word; a block polls its own group's
+      unsigned long long *rel = a.arrive_groups + (size_t)(kArriveGroups + tm.rank % groups) * kArriveStride;
+      if (s_last) {
+        for (int g = 0; g < groups; g++)
+          st_release_u64(a.arrive_groups + (size_t)(kArriveGroups + g) * kArriveStride, s_ep + 1);
+      } else {
+        long long spins = 0;
+        while (ld_acquire_u64(rel) < s_ep + 1) {
+#else
+      if (!s_last) {
+        long long spins = 0;
+        while (ld_acquire_u64(&a.sync->arrive) < target) {
+#endif
+          if (*((volatile int32_t *)&a.sync->abort)) break;
+          if (++spins > a.P.spin_limit) {
+            atomicExch(&a.sync->abort, 1);
+            break;
+          }
+#if PRIMA_POLL_SLEEP_NS > 0
+          __nanosleep(PRIMA_POLL_SLEEP_NS);
+#endif
+        }
+      }
+      if (*((volatile int32_t *)&a.sync->abort)) s_ok = 0;
+      s_ep += 1;
+      if (a.prof) {
+        const uint64_t now = global_timer_ns();
+        if (tm.rank < kProfBlocks && block_clock()[1]) a.prof->block_wait[phase == PH_B][tm.rank] += now - block_clock()[1];
+        block_clock()[0] = now;  // the next phase starts (after B: once decided)
+      }
+      if (a.prof && s_last) {  // the last arrival stands for the release
+        const uint64_t now = global_timer_ns(), tr = ldv(&a.prof->t_release);
+        if (tr) {
+          a.prof->phase_ns[phase & 7] += now - tr;
+          a.prof->phase_count[phase & 7] += 1;
+        }
+        a.prof->t_release = now;
+      }
+      if (phase == PH_A) snap.phase = PH_B;
+    }
+    __syncthreads();
+    if (!s_ok) {
+      if (hs.primed && threadIdx.x == 0) {  // leaving: let the staged copies land first (bounded)
+        constexpr int S = HotLayout<T>::kStages;
+        for (int u = 0; u < hs.issued; u++) {
+          mbar_wait(&hs.bars[u % S], (par >> (u % S)) & 1u);
+          par ^= 1u << (u % S);
+        }
+        hs.primed = 0;
+      }
+      return false;
+    }
+    if (phase == PH_B) {
+      const uint64_t t0 = (a.prof && tm.rank == 0 && threadIdx.x == 0) ? global_timer_ns() : 0;
+      decide<T>(a, snap, PH_B, tm, s_red);
+      __syncthreads();
+      if (t0) {
+        a.prof->decide_b_ns += global_timer_ns() - t0;
+        a.prof->decide_b_count += 1;
+        a.prof->decide_ns += global_timer_ns() - t0;
+      }
+      if (a.prof && threadIdx.x == 0) {
+        const uint64_t now = global_timer_ns();
+        if (tm.rank < kProfBlocks) a.prof->block_decide[tm.rank] += now - block_clock()[0];
+        block_clock()[0] = now;
+      }
+    }
+    return true;
+  }
   unsigned &s_gen = barrier_generation();
   __syncthreads();
   if (threadIdx.x == 0) {
     if (a.prof) {
       const uint64_t tr = ldv(&a.prof->t_release);
-      if (tr) atomicAdd((unsigned long long *)&a.prof->arrive_ns[phase & 7], (unsigned long long)(global_timer_ns() - tr));
+      if (tr) {
+        const unsigned long long d = global_timer_ns() - tr;
+        atomicAdd((unsigned long long *)&a.prof->arrive_ns[phase & 7], d);
+        if ((phase == PH_A || phase == PH_B) && tm.rank < kProfBlocks) {
+          a.prof->block_arrive[phase == PH_B][tm.rank] += d;  // this block's own slot
+          unsigned sm;
+          asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+          a.prof->block_sm[tm.rank] = (int32_t)sm;
+        }
+      }
     }
     const unsigned old = atom_add_acq_rel(&a.sync->count, 1u);
     s_last = old == (unsigned)(tm.nb - 1);
@@ -1440,23 +1652,15 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
       __threadfence();
       st_release(&a.sync->gen, s_gen + 1);
       s_gen += 1;
-    } else if (prime && threadIdx.x >> 5 == 1) {
-      prime_b();
-    } else if (list_a && threadIdx.x >> 5 == 1) {
-      list_tiles(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, hs);
     }
-  } else if (prime && threadIdx.x >> 5 == 1) {
-    prime_b();
-  } else if (list_a && threadIdx.x >> 5 == 1) {
-    list_tiles(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, hs);
   } else if (threadIdx.x == 0) {
-    unsigned long long spins = 0;
+    long long spins = 0;
     while (ld_acquire(&a.sync->gen) == s_gen) {
       if (*((volatile int32_t *)&a.sync->abort)) {
         s_ok = 0;
         break;
       }
-      if (++spins > kSpinLimit) {
+      if (++spins > a.P.spin_limit) {
         atomicExch(&a.sync->abort, 1);
         s_ok = 0;
         break;
@@ -1467,15 +1671,7 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     if (phase == PH_A) snap.phase = PH_B;
   }
   __syncthreads();
-  if (!s_ok && hs.primed && threadIdx.x == 0) {  // leaving: let the staged copies land first (bounded)
-    constexpr int S = HotLayout<T>::kStages;
-    for (int u = 0; u < hs.issued; u++) {
-      mbar_wait(&hs.bars[u % S], (par >> (u % S)) & 1u);
-      par ^= 1u << (u % S);
-    }
-    hs.primed = 0;
-  }
-  if (s_ok && phase != PH_A) load_control(a, snap);
+  if (s_ok) load_control(a, snap);
   return s_ok;
 }
 
@@ -1485,12 +1681,25 @@ template <typename T>
 __device__ __forceinline__ bool run_solve(const Args<T> &a, const Team &tm, Control &snap, HotShared &hs,
                                           unsigned &par, unsigned char *s_dyn) {
   T *s_prod = reinterpret_cast<T *>(s_dyn);
-  if (threadIdx.x == 0 && tm.nb > 1) barrier_generation() = ld_acquire(&a.sync->gen);
+  if (threadIdx.x == 0) {
+    hs.diag = a.sync->diag;
+    hs.prog = a.progress;
+  }
+  if (threadIdx.x == 0 && tm.nb > 1) {
+    barrier_generation() = ld_acquire(&a.sync->gen);
+    hot_epoch() = 0;  // the host zeroes the arrival counter before every solve
+    block_clock()[0] = block_clock()[1] = 0;
+  }
   load_control(a, snap);  // (syncs the block)
   bool alive = true;
   for (;;) {
     const int ph = snap.phase;
     if (ph == PH_DONE) break;
+    if (threadIdx.x == 0) {
+      progress(a.progress, 0, ph);
+      progress(a.progress, 1, (int32_t)snap.total_trials);
+      progress(a.progress, 9, snap.iteration);
+    }
     bool ok = true;
     switch (ph) {
       case PH_INIT: phase_init(a, snap, tm, s_prod); break;
@@ -1518,6 +1727,9 @@ __device__ __forceinline__ void init_stages(HotShared &hs) {
     fence_mbar_init();
     hs.primed = 0;
     hs.listed = nullptr;
+    hs.tag = 0;
+    hs.diag = nullptr;
+    hs.prog = nullptr;
   }
   __syncthreads();
 }
@@ -1602,7 +1814,7 @@ struct Layout {
 
 template <typename T>
 struct StateLayout {
-  size_t x[2], y[2], kx[2], xbar, kty, sx, sy, skx, skty, xr, yr, xo, yo, rco, part, ctl, sync, prof, bytes;
+  size_t x[2], y[2], kx[2], xbar, kty, sx, sy, skx, skty, xr, yr, xo, yo, rco, part, ctl, sync, groups, prof, bytes;
   size_t xa = 0, ya = 0, kxa = 0, ktya = 0, cw = 0, lw = 0, uw = 0, qw = 0, ylo = 0;
   StateLayout(int32_t n, int32_t m, int blocks, bool anchored) {
     Layout L;
@@ -1633,9 +1845,10 @@ struct StateLayout {
     xo = L.take<double>(n);
     rco = L.take<double>(n);
     yo = L.take<double>(m);
-    part = L.take<double>((int64_t)dev::kMaxQ * blocks);
+    part = L.take<double>((int64_t)dev::kSlots * blocks);
     ctl = L.take<dev::Control>(1);
     sync = L.take<dev::Sync>(1);
+    groups = L.take<unsigned long long>((int64_t)2 * dev::kArriveGroups * dev::kArriveStride);
     prof = L.take<dev::Prof>(1);
     bytes = L.off;
   }
@@ -1774,6 +1987,24 @@ bool phase_times() {
   return on;
 }
 
+// The progress record the kernel keeps when PRIMA_DEBUG_PROGRESS is set:
+// host-mapped memory the host reads while the kernel runs.
+volatile int32_t *progress_record(bool device_side) {
+  static int32_t *host = nullptr, *dev = nullptr;
+  static const bool on = std::getenv("PRIMA_DEBUG_PROGRESS") != nullptr;
+  if (!on) return nullptr;
+  if (!host) {
+    if (cudaHostAlloc((void **)&host, 256 * 16 * 4, cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void **)&dev, host, 0) != cudaSuccess) {
+      cudaGetLastError();
+      host = dev = nullptr;
+      return nullptr;
+    }
+    std::memset(host, 0, 256 * 16 * 4);
+  }
+  return device_side ? dev : host;
+}
+
 // Pdhg.Solve's initialise (Pdhg.scala:250-309) on the host -- the opening
 // step, primal weight and the projected start point -- and the Args, Control
 // and Sync records, with the iterate state at `base` laid out as S.
@@ -1869,6 +2100,7 @@ int32_t setup_job(Ctx *c, Job<T> &j, char *base, const StateLayout<T> &S, int bl
   a.tiles_t = (const int2 *)L.b_tiles[w][1].ptr;
   a.ntiles_k = L.ntiles[w][0];
   a.ntiles_t = L.ntiles[w][1];
+
   if (anchored) {
     a.anchored = 1;
     a.xa = (double *)(base + S.xa);
@@ -1906,6 +2138,9 @@ int32_t setup_job(Ctx *c, Job<T> &j, char *base, const StateLayout<T> &S, int bl
   std::memset(&sync, 0, sizeof(sync));
   PRIMA_CUDA_TRY(cudaMemcpyAsync(a.ctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
   PRIMA_CUDA_TRY(cudaMemcpyAsync(a.sync, &sync, sizeof(sync), cudaMemcpyHostToDevice, s));
+  a.arrive_groups = (unsigned long long *)(base + S.groups);
+  PRIMA_CUDA_TRY(cudaMemsetAsync(a.arrive_groups, 0,
+                                 sizeof(unsigned long long) * 2 * dev::kArriveGroups * dev::kArriveStride, s));
   if (a.prof) PRIMA_CUDA_TRY(cudaMemsetAsync(a.prof, 0, sizeof(dev::Prof), s));
 
   dev::Params &P = a.P;
@@ -1924,7 +2159,9 @@ int32_t setup_job(Ctx *c, Job<T> &j, char *base, const StateLayout<T> &S, int bl
   P.matrix_norm = L.orig_spectral_bound;
   P.offset = L.host ? L.host->objective_offset : 0.0;
   P.round_rho = anchored ? req.round_rho : 0.0;
+  P.spin_limit = c->wait_limit > 0 ? (long long)c->wait_limit : dev::kDefaultSpinLimit;
   a.cancel = c->cancel_mapped_dev;
+  a.progress = progress_record(true);
   PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
   j.setup_ms = ms_since(j.t0);
   P.setup_ms = j.setup_ms;
@@ -1962,6 +2199,7 @@ int32_t finish_job(Ctx * /*c*/, Job<T> &j, float kms, int blocks) {
   info->setup_ms = j.setup_ms;
   info->trials = ctl.total_trials;
   info->solve_ms = (int64_t)ms_since(j.t0);
+  info->blocks = blocks;
   if (req.rounds) *req.rounds = ctl.rounds;
   if (a.prof) {
     dev::Prof prof;
@@ -1985,17 +2223,85 @@ int32_t finish_job(Ctx * /*c*/, Job<T> &j, float kms, int blocks) {
         std::fprintf(stderr, " %s %.2f us x%lld", names[k], 1e-3 * (double)prof.phase_ns[k] / (double)prof.phase_count[k],
                      (long long)prof.phase_count[k]);
     std::fprintf(stderr, "\n");
+    // per-block arrival spread: the slowest blocks, their SMs and tile counts
+    const int nbp = std::min(blocks, dev::kProfBlocks);
+    for (int ph = 0; ph < 2 && nbp > 1; ph++) {
+      const int64_t cnt = prof.phase_count[ph == 0 ? dev::PH_A : dev::PH_B];
+      if (!cnt) continue;
+      std::vector<std::pair<double, int>> v;
+      for (int b = 0; b < nbp; b++) v.push_back({1e-3 * (double)prof.block_arrive[ph][b] / (double)cnt, b});
+      std::sort(v.begin(), v.end());
+      const int32_t nt = ph == 0 ? a.ntiles_t : a.ntiles_k;
+      auto tiles_of = [&](int b) { return b < nt ? (nt - b + blocks - 1) / blocks : 0; };
+      std::fprintf(stderr, "[prima] phase %s arrival per block: min %.2f p10 %.2f median %.2f p90 %.2f max %.2f us; slowest:",
+                   ph == 0 ? "A" : "B", v.front().first, v[nbp / 10].first, v[nbp / 2].first, v[(9 * nbp) / 10].first,
+                   v.back().first);
+      for (int k = 0; k < 8 && k < nbp; k++) {
+        const int b = v[nbp - 1 - k].second;
+        std::fprintf(stderr, " b%d(sm%d,%dt)=%.2f", b, prof.block_sm[b], tiles_of(b), v[nbp - 1 - k].first);
+      }
+      std::fprintf(stderr, " fastest:");
+      for (int k = 0; k < 4 && k < nbp; k++) {
+        const int b = v[k].second;
+        std::fprintf(stderr, " b%d(sm%d,%dt)=%.2f", b, prof.block_sm[b], tiles_of(b), v[k].first);
+      }
+      {  // the phase's own work, the barrier wait and (after B) the decision, per block
+        double wsum = 0, wmax = 0, tsum = 0, dsum = 0;
+        for (int b = 0; b < nbp; b++) {
+          const double w = 1e-3 * (double)prof.block_work[ph][b] / (double)cnt;
+          wsum += w;
+          wmax = std::max(wmax, w);
+          tsum += 1e-3 * (double)prof.block_wait[ph][b] / (double)cnt;
+          if (ph == 1) dsum += 1e-3 * (double)prof.block_decide[b] / (double)cnt;
+        }
+        std::fprintf(stderr, " | work mean %.2f max %.2f, barrier wait mean %.2f", wsum / nbp, wmax, tsum / nbp);
+        if (ph == 1) std::fprintf(stderr, ", decision mean %.2f", dsum / nbp);
+      }
+      // mean arrival by SM group of 8 consecutive SM ids (a GPC-sized bucket)
+      double by[32] = {0};
+      int nby[32] = {0};
+      for (int b = 0; b < nbp; b++) {
+        const int g = std::min(31, std::max(0, prof.block_sm[b] / 8));
+        by[g] += 1e-3 * (double)prof.block_arrive[ph][b] / (double)cnt;
+        nby[g]++;
+      }
+      std::fprintf(stderr, " | by sm/8:");
+      for (int g = 0; g < 32; g++)
+        if (nby[g]) std::fprintf(stderr, " %.1f", by[g] / nby[g]);
+      std::fprintf(stderr, "\n");
+    }
   }
   if (ctl.error) {
-    set_error("a bounded device-side wait gave up; the solve was abandoned");
+    std::string msg = "a bounded device-side wait gave up; the solve was abandoned";
+    if (sync.diag[0]) {
+      static const char *tags[4] = {"?", "phase A", "phase B", "SpMV"};
+      char buf[256];
+      std::snprintf(buf, sizeof(buf), " (first failure: a %s stage wait, stage %d, parity %d, tile %d of %d, block %d)",
+                    tags[sync.diag[1] & 3], sync.diag[3], sync.diag[4], sync.diag[5], sync.diag[6], sync.diag[7]);
+      msg += buf;
+    }
+    set_error(msg);
     return PRIMA_ERR_TIMEOUT;
   }
   return PRIMA_OK;
 }
 
+void print_progress() {
+  volatile int32_t *p = progress_record(false);
+  if (!p) return;
+  std::fprintf(stderr, "[prima progress]");
+  for (int b = 0; b < 4; b++) {
+    std::fprintf(stderr, " | b%d:", b);
+    for (int w = 0; w < 10; w++) std::fprintf(stderr, " %d", p[b * 16 + w]);
+  }
+  std::fprintf(stderr, "\n");
+  std::fflush(stderr);
+}
+
 // Waits for the event ending a launch, forwarding the caller's cancel flag
 // to the mapped flag the device polls at evaluation points.
 int32_t wait_forwarding_cancel(Ctx *c, cudaEvent_t done, const volatile int32_t *cancel) {
+  auto last = Clock::now();
   for (int spin = 0;; spin++) {
     const cudaError_t q = cudaEventQuery(done);
     if (q == cudaSuccess) return PRIMA_OK;
@@ -2005,6 +2311,10 @@ int32_t wait_forwarding_cancel(Ctx *c, cudaEvent_t done, const volatile int32_t 
     }
     if (cancel && *cancel) *(volatile int32_t *)c->cancel_mapped = 1;
     if (spin > 200) std::this_thread::sleep_for(std::chrono::microseconds(20));
+    if (progress_record(false) && ms_since(last) > 2000.0) {
+      print_progress();
+      last = Clock::now();
+    }
   }
 }
 
@@ -2533,6 +2843,26 @@ extern "C" int32_t prima_problem_set_bounds(prima_handle ctx, prima_handle probl
   h.lp.lower = h.lower.data();
   h.lp.upper = h.upper.data();
   return L.set_bounds(lower, upper, c->stream);
+}
+
+extern "C" int32_t prima_problem_scaled(prima_handle ctx, prima_handle problem, double *values, double *objective,
+                                        double *rhs, double *lower, double *upper, double *row_scale,
+                                        double *col_scale) {
+  CTX_OR_RETURN(ctx);
+  auto it = c->problems.find(problem);
+  if (it == c->problems.end()) return (set_error("unknown problem handle"), PRIMA_ERR_CLOSED);
+  const PreparedLp &L = *it->second;
+  const struct {
+    double *dst;
+    const void *src;
+    int64_t count;
+  } outs[] = {{values, L.kv(), L.nnz}, {objective, L.sc(), L.n}, {rhs, L.sq(), L.m}, {lower, L.sl(), L.n},
+              {upper, L.su(), L.n}, {row_scale, L.rs(), L.m}, {col_scale, L.cs(), L.n}};
+  for (const auto &o : outs)
+    if (o.dst && o.count > 0)
+      PRIMA_CUDA_TRY(cudaMemcpyAsync(o.dst, o.src, (size_t)o.count * 8, cudaMemcpyDeviceToHost, c->stream));
+  PRIMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return PRIMA_OK;
 }
 
 extern "C" int32_t prima_problem_solve(prima_handle ctx, prima_handle problem, const prima_params *params,

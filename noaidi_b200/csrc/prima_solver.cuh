@@ -56,6 +56,13 @@ constexpr int kTileRows = 512;      // rows of one CSR-stream tile (2 per thread
 constexpr int kRowsPerThread = kTileRows / kThreads;
 constexpr int kTileCap = 4096;      // staged products per tile (dynamic shared memory)
 constexpr int kMaxQ = 17;
+// Global block partials: slots [0, kMaxQ) for the cold phases, then two
+// banks of kHotQ slots for the trial (phase A: DX, phase B: DY, INTER), used
+// by alternate trials so that a block still reading one trial's partials is
+// never overwritten by a faster block already in the next trial.
+constexpr int kHotQ = 3;
+constexpr int kSlots = kMaxQ + 2 * kHotQ;
+__host__ __device__ constexpr int hot_bank(int64_t trial) { return kMaxQ + (int)(trial & 1) * kHotQ; }
 
 enum : int { PH_INIT = 0, PH_A = 1, PH_B = 2, PH_F = 3, PH_R = 4, PH_W = 5, PH_DONE = 6, PH_R2 = 7 };
 enum : int { F_FIXPOINT = 0, F_CHECKPOINT = 1, F_ITERLIMIT = 2 };
@@ -101,6 +108,7 @@ struct Params {
   double matrix_norm;  // spectral bound of the ORIGINAL matrix (certificates)
   double offset;
   double round_rho;  // anchored mode: a checkpoint this far below the round's start error opens a new round
+  long long spin_limit;  // team-barrier polls before a block gives up and raises the abort flag
 };
 
 // Published by the deciding block at every barrier.
@@ -119,12 +127,22 @@ struct Control {
   Kkt current, average, final_kkt;
 };
 
+// Hot barriers count arrivals in two levels, so that no one address takes
+// every block's atomic: block `rank` counts itself in on group rank % G's
+// counter, and the last block of each group on the team's counter.
+constexpr int kArriveGroups = 32;     // G, at most
+constexpr int kArriveStride = 16;     // counters 128 bytes apart (u64 words)
+
 struct Sync {
-  unsigned int count;
-  unsigned int gen;
+  unsigned int count;   // cold barriers: arrivals so far (reset by the deciding block)
+  unsigned int gen;     // cold barriers: released generations
   int32_t abort;
   int32_t pad;
+  unsigned long long arrive;  // hot barriers: groups complete so far in the solve, never reset
+  int32_t diag[8];            // where a bounded stage wait gave up (zero: none did)
 };
+
+constexpr int kProfBlocks = 1024;  // blocks whose own arrival times the phase record keeps
 
 // Phase timing, kept by whichever block decides (one at a time): time from a
 // barrier's release to the last block's arrival at the next one, per phase
@@ -140,6 +158,14 @@ struct Prof {
   uint64_t decide_b_ns, reduce_b_ns;
   int64_t decide_b_count;
   uint64_t arrive_ns[8];  // every block's arrival after the release, summed
+  // per block: arrival after the release in phases A and B, summed over the
+  // trials, and the SM the block runs on (is the spread systematic?)
+  uint64_t block_arrive[2][kProfBlocks];
+  int32_t block_sm[kProfBlocks];
+  // per block, summed over the trials: the phase's own work (its start to its
+  // arrival), the wait at the barrier (arrival to seeing the team complete)
+  // and, after phase B, the decision (seeing the team complete to starting A)
+  uint64_t block_work[2][kProfBlocks], block_wait[2][kProfBlocks], block_decide[kProfBlocks];
 };
 
 template <typename T>
@@ -159,7 +185,7 @@ struct Args {
   T *xbar, *kty, *sx, *sy, *skx, *skty, *xr, *yr;
   // solution in the caller's units
   double *xo, *yo, *rco;
-  double *partials;  // [kMaxQ][max_blocks]
+  double *partials;  // [kSlots][max_blocks]
   int32_t max_blocks, anchored;
   const int2 *tiles_k, *tiles_t;  // tile tables of K and K': (first row, first nonzero), + a sentinel
   int32_t ntiles_k, ntiles_t;
@@ -181,6 +207,11 @@ struct Args {
   // a single solve.
   int32_t *queue, *team_next;
   int32_t team, pad2;
+  // PRIMA_DEBUG_PROGRESS: host-mapped progress record, 16 words per block
+  // (phase, trial, producer fill / own / state, consumer stage / state,
+  // barrier state, iteration), readable while the kernel runs; else nullptr
+  volatile int32_t *progress;
+  unsigned long long *arrive_groups;  // hot barriers: per-group arrival counters, then release words [2G * kArriveStride]
   Params P;
 };
 

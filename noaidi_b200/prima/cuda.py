@@ -26,7 +26,10 @@ from .model import LpProblem, SparseMatrix
 from .types import (KktError, LpSolution, MixedPrecisionParams, MixedPrecisionResult, PdhgParams, SolveStatus,
                     WarmStart)
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "libprima_cuda.so")
+# The in-tree build; PRIMA_CUDA_LIBRARY names another build of the same ABI
+# (a differently tuned compile of the same sources, say).
+LIB_PATH = os.environ.get("PRIMA_CUDA_LIBRARY") or \
+    os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "libprima_cuda.so")
 
 OK, ERR_INVALID_ARGUMENT, ERR_OUT_OF_MEMORY, ERR_CUDA, ERR_TIMEOUT, ERR_CLOSED, ERR_NO_DEVICE, ERR_PARSE = range(8)
 MIXED_TWO_PASS, MIXED_REFINEMENT = 0, 1
@@ -70,7 +73,8 @@ class CInfo(C.Structure):
                 ("device_error", C.c_int32), ("solve_ms", C.c_int64), ("objective", C.c_double),
                 ("dual_objective", C.c_double), ("primal_residual", C.c_double), ("dual_residual", C.c_double),
                 ("final_step_size", C.c_double), ("final_primal_weight", C.c_double), ("device_ms", C.c_double),
-                ("setup_ms", C.c_double), ("trials", C.c_int64), ("span_ms", C.c_double)]
+                ("setup_ms", C.c_double), ("trials", C.c_int64), ("span_ms", C.c_double), ("blocks", C.c_int32),
+                ("pad2", C.c_int32)]
 
 
 class CMixedParams(C.Structure):
@@ -108,6 +112,7 @@ SIGNATURES = {
     "prima_open": (C.c_int32, [C.c_int32, C.c_int32, _HP]),
     "prima_close": (C.c_int32, [_H]),
     "prima_capabilities_get": (C.c_int32, [_H, C.POINTER(Capabilities)]),
+    "prima_set_device_wait_limit": (C.c_int32, [_H, C.c_int64]),
     "prima_vec_alloc": (C.c_int32, [_H, C.c_int64, _HP]),
     "prima_vec_upload": (C.c_int32, [_H, _DP, C.c_int64, _HP]),
     "prima_vec_download": (C.c_int32, [_H, _H, _DP, C.c_int64]),
@@ -137,6 +142,7 @@ SIGNATURES = {
     "prima_problem_create": (C.c_int32, [_H, C.POINTER(CLp), C.POINTER(CParams), _HP]),
     "prima_problem_free": (C.c_int32, [_H, _H]),
     "prima_problem_set_bounds": (C.c_int32, [_H, _H, _DP, _DP]),
+    "prima_problem_scaled": (C.c_int32, [_H, _H, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
     "prima_problem_solve": (C.c_int32, [_H, _H, C.POINTER(CParams), C.POINTER(CWarm), _IP, _DP, _DP, _DP,
                                         C.POINTER(CInfo)]),
     "prima_problem_mixed_solve": (C.c_int32, [_H, _H, C.POINTER(CParams), C.POINTER(CMixedParams), _IP, _DP, _DP,
@@ -247,6 +253,11 @@ class Context:
         if not self._closed:
             _check(self.lib.prima_close(self.handle))
             self._closed = True
+
+    def set_device_wait_limit(self, polls: int) -> None:
+        """Team-barrier polls before a block of a solve gives up
+        (``prima_set_device_wait_limit``); 0 restores the default."""
+        _check(self.lib.prima_set_device_wait_limit(self.handle, polls))
 
     def __enter__(self):
         return self
@@ -365,6 +376,7 @@ def _solution(info: CInfo, x, y, rc) -> LpSolution:
     sol.setup_ms = info.setup_ms
     sol.trials = info.trials
     sol.span_ms = info.span_ms
+    sol.blocks = info.blocks
     return sol
 
 
@@ -537,6 +549,16 @@ class DeviceProblem:
         return MixedPrecisionResult(_solution(info, x, y, rc), minfo.reduced_iterations, minfo.reduced_restarts,
                                     int(minfo.reduced_ms), minfo.refinement_iterations, int(minfo.refinement_ms),
                                     bool(minfo.refined), minfo.refinement_rounds)
+
+    def scaled(self):
+        """The device's equilibration of this problem (``prima_problem_scaled``):
+        (values in CSR order, objective, rhs, lower, upper, row scale, column
+        scale), all float64."""
+        p = self.problem
+        n, m, nnz = p.num_variables, p.num_constraints, p.constraint_matrix.nnz
+        out = (np.zeros(nnz), np.zeros(n), np.zeros(m), np.zeros(n), np.zeros(n), np.zeros(m), np.zeros(n))
+        _check(self.ctx.lib.prima_problem_scaled(self.ctx.handle, self.handle, *[_dp(a) for a in out]))
+        return out
 
     def free(self) -> None:
         if self.handle is not None and not self.ctx._closed:

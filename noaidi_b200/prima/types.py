@@ -231,10 +231,13 @@ class WarmStart:
 
     def save(self, path: str) -> None:
         """The four-tuple to disk (numpy .npz), exactly: a solve resumed from
-        ``load(path)`` is the one resumed from this object."""
-        np.savez(path, primal=self.primal, dual=self.dual,
-                 step_size=np.float64(math.nan if self.step_size is None else self.step_size),
-                 primal_weight=np.float64(math.nan if self.primal_weight is None else self.primal_weight))
+        ``load(path)`` is the one resumed from this object.  The file lands
+        at ``path`` exactly (through a file handle, so numpy adds no
+        ``.npz`` suffix)."""
+        with open(path, "wb") as f:
+            np.savez(f, primal=self.primal, dual=self.dual,
+                     step_size=np.float64(math.nan if self.step_size is None else self.step_size),
+                     primal_weight=np.float64(math.nan if self.primal_weight is None else self.primal_weight))
 
     @staticmethod
     def load(path: str) -> "WarmStart":

@@ -7,7 +7,7 @@ distribution factors and its island split) from the reference's
 goldens (reference/goldens/{networks,results} in oluies/noaidi, generated by
 PyPSA 1.2.4) into tests/golden/lopf/<network>/.
 
-    python tests/golden/make_lopf_fixtures.py [path to the reference checkout]
+    python tests/golden/make_lopf_fixtures.py <path to the reference checkout>
 """
 import json
 import os
@@ -106,4 +106,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_lopf_fixtures.py <path to the reference checkout>")
+    main(sys.argv[1])

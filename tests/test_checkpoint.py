@@ -31,3 +31,13 @@ def test_a_point_without_adaptive_state_round_trips(tmp_path):
     back = WarmStart.load(path)
     assert back.step_size is None and back.primal_weight is None
     assert np.array_equal(back.primal, warm.primal)
+
+
+def test_a_path_without_extension_is_written_and_read_at_that_path(tmp_path):
+    warm = WarmStart(np.array([3.0, -1.0]), np.array([0.25, 4.0]), 0.5, 2.0)
+    path = str(tmp_path / "ckpt")
+    warm.save(path)
+    assert (tmp_path / "ckpt").exists() and not (tmp_path / "ckpt.npz").exists()
+    back = WarmStart.load(path)
+    assert np.array_equal(back.primal, warm.primal) and np.array_equal(back.dual, warm.dual)
+    assert (back.step_size, back.primal_weight) == (0.5, 2.0)

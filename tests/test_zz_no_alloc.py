@@ -51,8 +51,13 @@ def test_matches_prima_dot_on_consecutive_calls(bits):
         xd = torch.from_numpy(x).to(device="cuda:0", dtype=dtype)
         yd = torch.from_numpy(y).to(device="cuda:0", dtype=dtype)
         got = _no_alloc_dot(lib, xd, yd, bits, stream)
-        scale = float(np.abs(xd.double().cpu().numpy() * yd.double().cpu().numpy()).sum())
+        xr, yr = xd.double().cpu().numpy(), yd.double().cpu().numpy()  # the inputs as the device holds them
+        scale = float(np.abs(xr * yr).sum())
         assert abs(got - want) <= 1e-9 * scale, (n, got, want)
+        # and, independently of the library, a float64 sum on the host of the
+        # same (rounded) inputs
+        host = float(np.dot(xr, yr))
+        assert abs(got - host) <= 1e-9 * scale, (n, got, host)
 
 
 @pytest.mark.gpu
@@ -72,3 +77,27 @@ def test_empty_and_oversized_inputs():
     assert b"16777216" in lib.prima_last_error()
     rc = lib.prima_dot_no_alloc(_ptr(x), _ptr(x), 4, 16, _ptr(out), C.c_void_p(stream.cuda_stream))
     assert rc == cuda.ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.gpu
+def test_host_memory_is_refused_before_any_launch():
+    """The arrays come from the caller; a host buffer handed over by mistake
+    is refused (nothing is queued that would read it), and a device call on
+    the same stream works afterwards."""
+    import torch
+    lib = cuda.library()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    host = np.ones(1024, dtype=np.float64)
+    xd = torch.ones(1024, dtype=torch.float64, device="cuda:0")
+    out = torch.full((1,), 7.0, dtype=torch.float64, device="cuda:0")
+    host_out = np.zeros(1)
+    hp = C.c_void_p(host.ctypes.data)
+    for x, y, o in ((hp, _ptr(xd), _ptr(out)), (_ptr(xd), hp, _ptr(out)),
+                    (_ptr(xd), _ptr(xd), C.c_void_p(host_out.ctypes.data))):
+        rc = lib.prima_dot_no_alloc(x, y, 1024, 64, o, C.c_void_p(stream.cuda_stream))
+        assert rc == cuda.ERR_INVALID_ARGUMENT
+        assert b"current device" in lib.prima_last_error()
+    stream.synchronize()
+    assert out.item() == 7.0
+    assert _no_alloc_dot(lib, xd, xd, 64, stream) == 1024.0
