@@ -22,3 +22,22 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["workload"].startswith("dc-lopf")
+    # the same config as the device arm, with the shape of the instance
+    assert (d["config"]["n"], d["config"]["m"], d["config"]["nnz"]) == (1_344_000, 840_000, 3_024_000)
+    assert d["cpu_baseline"]["extrapolated"] is True and "EXTRAPOLATED" in d["cpu_baseline"]["sample"]
+    assert d["cpu_baseline"]["host_cores"] >= 1
+    c1 = d["config1_measured"]
+    assert c1["status"] == "OPTIMAL" and c1["time_to_tolerance_s"] > 0 and c1["iterations"] > 0
+
+
+def test_highs_fixture_still_describes_the_bench_instances():
+    """tests/golden/bench_highs.json holds HiGHS's optimum of the bench
+    workload per seed; the generator must still build those exact bytes."""
+    sys.path.insert(0, ROOT)
+    from noaidi_b200.prima import generators as G
+    from noaidi_b200.prima.generators import problem_hash
+    fix = json.load(open(os.path.join(ROOT, "tests", "golden", "bench_highs.json")))
+    assert {"0", "1", "2"} <= set(fix)
+    p = G.dc_lopf(seed=0, buses=2000, lines=3000, generators=1000, snapshots=168)
+    assert problem_hash(p) == fix["0"]["hash"]
+    assert fix["0"]["highs_objective"] > 0
