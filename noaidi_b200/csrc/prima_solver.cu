@@ -44,14 +44,14 @@ __device__ __forceinline__ unsigned long long atom_add_acq_rel_u64(unsigned long
   asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
   return old;
 }
-__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
+// Phase A's first tiles are staged during the barrier after phase B on the
+// guess that the trial is accepted (see barrier_decide); 0 stages its tile
+// list only.
+#ifndef PRIMA_SPEC_A
+#define PRIMA_SPEC_A 1
+#endif
 #ifndef PRIMA_POLL_SLEEP_NS
 #define PRIMA_POLL_SLEEP_NS 32
-#endif
-#ifndef PRIMA_GROUP_RELEASE
-#define PRIMA_GROUP_RELEASE 0
 #endif
 __device__ __forceinline__ uint64_t global_timer_ns() {
   uint64_t t;
@@ -171,7 +171,8 @@ template <>
 struct Hot<double> : HotShape<PRIMA_HOT_F64_CAP, PRIMA_HOT_F64_STAGES, PRIMA_HOT_F64_RPT> {};
 template <typename T>
 constexpr int kHotRows = kThreads * Hot<T>::kRowsPerThread;  // rows per tile, at most
-constexpr int kHotVec = 6;          // vector slices per tile, at most
+constexpr int kHotVec = 6;          // vector operands per row, at most
+
 constexpr int kHotBatch = 128;      // tiles whose table entries a block stages at once
 constexpr int kMaxStages = Hot<float>::kStages > Hot<double>::kStages ? Hot<float>::kStages : Hot<double>::kStages;
 
@@ -279,10 +280,10 @@ struct HotShared {
 };
 
 // The tile engine over a table of ntiles tiles (see above).  rp == nullptr:
-// no SpMV, vectors only.  epi(r, i, acc, slices) runs on the thread of row i
+// no SpMV, vectors only.  epi(r, i, acc, vals) runs on the thread of row i
 // of the tile (row r of the matrix): acc is the row's product (an
-// index-order sum from zero, as csr_tiles), slices the tile's vector slices
-// (stride kHotRows).  Returns false, uniformly over the block, when the
+// index-order sum from zero, as csr_tiles), vals the row's vector operands
+// (vecs[k][r] for k < nv).  Returns false, uniformly over the block, when the
 // team's abort flag is up.
 // Issue tile j of the batch staged in hs.tiles into stage j % kStages: its
 // vector slices and, for an SpMV, its row pointers, column indices and
@@ -422,6 +423,14 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
       // each thread takes rows threadIdx.x + r * kThreads of the tile; the
       // first four gathers of all its rows are issued together
       constexpr int RPT = Hot<T>::kRowsPerThread;
+      // the vector operands of the thread's rows, from the stage
+      T vv[RPT][kHotVec];
+#pragma unroll
+      for (int q = 0; q < RPT; q++) {
+        const int i = threadIdx.x + q * kThreads;
+#pragma unroll
+        for (int k = 0; k < kHotVec; k++) vv[q][k] = (k < nv && i < rows) ? slices[k * kHotRows<T> + i] : T(0);
+      }
       T acc[RPT];
       int32_t a0[RPT], a1[RPT];
 #pragma unroll
@@ -515,13 +524,19 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
               for (int32_t k = 0; k < cnt; k++) accw = accw + scratch[k];
             __syncwarp();
           }
-          if (lane == 0) epi(r0 + w, w, accw, slices);
+          if (lane == 0) {
+            T vw[kHotVec];
+#pragma unroll
+            for (int k = 0; k < kHotVec; k++)
+              vw[k] = k < nv ? slices[k * kHotRows<T> + w] : T(0);
+            epi(r0 + w, w, accw, vw);
+          }
         }
       } else {
 #pragma unroll
         for (int q = 0; q < RPT; q++) {
           const int i = threadIdx.x + q * kThreads;
-          if (i < rows) epi(r0 + i, i, acc[q], slices);
+          if (i < rows) epi(r0 + i, i, acc[q], vv[q]);
         }
       }
       // the last warp done with this stage refills it with the tile S further on
@@ -947,10 +962,8 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
   if (s.pend) {
     const T *vecs[6] = {x, a.sx, a.skty, a.c, a.l, a.u};
     ok = hot_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, a.tp, a.tci, a.tv, (const T *)a.y[s.yc], vecs, 6, smem, hs, par,
-                      &a.sync->abort, 1, [&](int32_t j, int i, T kt, const T *sl) {
-                        constexpr int S = kHotRows<T>;
-                        const T xj = sl[i], sx = sl[S + i], skt = sl[2 * S + i];
-                        const T cj = sl[3 * S + i], lj = sl[4 * S + i], uj = sl[5 * S + i];
+                      &a.sync->abort, 1, [&](int32_t j, int, T kt, const T *vv) {
+                        const T xj = vv[0], sx = vv[1], skt = vv[2], cj = vv[3], lj = vv[4], uj = vv[5];
                         a.kty[j] = kt;
                         a.sx[j] = (w * xj) + (T(1) * sx);
                         a.skty[j] = (w * kt) + (T(1) * skt);
@@ -959,9 +972,8 @@ __device__ bool phase_a(const Args<T> &a, const Control &s, const Team &tm, unsi
   } else {
     const T *vecs[5] = {x, a.kty, a.c, a.l, a.u};
     ok = hot_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, nullptr, nullptr, nullptr, nullptr, vecs, 5, smem, hs, par,
-                      &a.sync->abort, 1, [&](int32_t j, int i, T, const T *sl) {
-                        constexpr int S = kHotRows<T>;
-                        step(j, sl[i], sl[S + i], sl[2 * S + i], sl[3 * S + i], sl[4 * S + i]);
+                      &a.sync->abort, 1, [&](int32_t j, int, T, const T *vv) {
+                        step(j, vv[0], vv[1], vv[2], vv[3], vv[4]);
                       });
   }
   block_partials<1>(v, a.partials, a.max_blocks, tm.rank, tm.nb, Q_DX, tm.s_part, hot_bank(s.total_trials) + Q_DX);
@@ -999,11 +1011,10 @@ __device__ bool phase_b(const Args<T> &a, const Control &s, const Team &tm, unsi
   const int iylo = pend ? 5 : 3;
   const bool has_lo = a.ylo != nullptr;
   const bool ok = hot_tiles<T>(a.ntiles_k, tm.nb, tm.rank, a.tiles_k, a.kp, a.kci, a.kv, (const T *)a.xbar, vecs, nv, smem, hs, par,
-                               &a.sync->abort, 2, [&](int32_t r, int i, T kb, const T *sl) {
-    constexpr int S = kHotRows<T>;
-    const T yr = sl[i], kxr = sl[S + i], qr = sl[2 * S + i];
-    const T syr = pend ? sl[3 * S + i] : T(0), skxr = pend ? sl[4 * S + i] : T(0);
-    const T lb = has_lo ? sl[iylo * S + i] : T(0);
+                               &a.sync->abort, 2, [&](int32_t r, int, T kb, const T *vv) {
+    const T yr = vv[0], kxr = vv[1], qr = vv[2];
+    const T syr = pend ? vv[3] : T(0), skxr = pend ? vv[4] : T(0);
+    const T lb = has_lo ? vv[iylo] : T(0);
     if (pend) {
       a.sy[r] = (w * yr) + (T(1) * syr);
       a.skx[r] = (w * kxr) + (T(1) * skxr);
@@ -1447,7 +1458,17 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     const int nv = b_operands(a, snap, vecs);
     prime_tiles<T>(a.ntiles_k, tm.nb, tm.rank, a.tiles_k, a.kp, a.kci, a.kv, vecs, nv, smem, hs);
   };
-  auto list_a_tiles = [&] { list_tiles(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, hs); };
+  auto list_a_tiles = [&] {
+#if PRIMA_SPEC_A
+    // nearly every trial is accepted: stage A's first tiles as an accepted
+    // trial's phase A reads them (the new x, the pending commit's sums and
+    // K'); a decision that goes elsewhere lets them land and drops them
+    const T *vecs[6] = {a.x[snap.xc ^ 1], a.sx, a.skty, a.c, a.l, a.u};
+    prime_tiles<T>(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, a.tp, a.tci, a.tv, vecs, 6, smem, hs);
+#else
+    list_tiles(a.ntiles_t, tm.nb, tm.rank, a.tiles_t, hs);
+#endif
+  };
   __shared__ int s_last, s_ok;
   __shared__ double s_red[kMaxQ];
   if (tm.nb == 1) {
@@ -1527,20 +1548,9 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
       list_a_tiles();
     } else if (threadIdx.x == 0) {
       const unsigned long long target = (s_ep + 1) * (unsigned long long)groups;
-#if PRIMA_GROUP_RELEASE
-      // the team's last block writes every group's release word; a block polls its own group's
-      unsigned long long *rel = a.arrive_groups + (size_t)(kArriveGroups + tm.rank % groups) * kArriveStride;
-      if (s_last) {
-        for (int g = 0; g < groups; g++)
-          st_release_u64(a.arrive_groups + (size_t)(kArriveGroups + g) * kArriveStride, s_ep + 1);
-      } else {
-        long long spins = 0;
-        while (ld_acquire_u64(rel) < s_ep + 1) {
-#else
       if (!s_last) {
         long long spins = 0;
         while (ld_acquire_u64(&a.sync->arrive) < target) {
-#endif
           if (*((volatile int32_t *)&a.sync->abort)) break;
           if (++spins > a.P.spin_limit) {
             atomicExch(&a.sync->abort, 1);
@@ -1584,6 +1594,20 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
       const uint64_t t0 = (a.prof && tm.rank == 0 && threadIdx.x == 0) ? global_timer_ns() : 0;
       decide<T>(a, snap, PH_B, tm, s_red);
       __syncthreads();
+#if PRIMA_SPEC_A
+      if (hs.primed && !(snap.phase == PH_A && snap.pend)) {
+        // the staged tiles were for an accepted trial's phase A: let their
+        // bytes land (bounded), then drop them
+        constexpr int S = HotLayout<T>::kStages;
+        const int issued = hs.issued;
+        if (threadIdx.x == 0)
+          for (int u = 0; u < issued; u++) mbar_wait(&hs.bars[u % S], (par >> (u % S)) & 1u);
+        __syncthreads();
+        for (int u = 0; u < issued; u++) par ^= 1u << (u % S);
+        if (threadIdx.x == 0) hs.primed = 0;
+        __syncthreads();
+      }
+#endif
       if (t0) {
         a.prof->decide_b_ns += global_timer_ns() - t0;
         a.prof->decide_b_count += 1;
@@ -1848,7 +1872,7 @@ struct StateLayout {
     part = L.take<double>((int64_t)dev::kSlots * blocks);
     ctl = L.take<dev::Control>(1);
     sync = L.take<dev::Sync>(1);
-    groups = L.take<unsigned long long>((int64_t)2 * dev::kArriveGroups * dev::kArriveStride);
+    groups = L.take<unsigned long long>((int64_t)dev::kArriveGroups * dev::kArriveStride);
     prof = L.take<dev::Prof>(1);
     bytes = L.off;
   }
@@ -2140,7 +2164,7 @@ int32_t setup_job(Ctx *c, Job<T> &j, char *base, const StateLayout<T> &S, int bl
   PRIMA_CUDA_TRY(cudaMemcpyAsync(a.sync, &sync, sizeof(sync), cudaMemcpyHostToDevice, s));
   a.arrive_groups = (unsigned long long *)(base + S.groups);
   PRIMA_CUDA_TRY(cudaMemsetAsync(a.arrive_groups, 0,
-                                 sizeof(unsigned long long) * 2 * dev::kArriveGroups * dev::kArriveStride, s));
+                                 sizeof(unsigned long long) * dev::kArriveGroups * dev::kArriveStride, s));
   if (a.prof) PRIMA_CUDA_TRY(cudaMemsetAsync(a.prof, 0, sizeof(dev::Prof), s));
 
   dev::Params &P = a.P;

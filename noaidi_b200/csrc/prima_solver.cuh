@@ -211,7 +211,7 @@ struct Args {
   // (phase, trial, producer fill / own / state, consumer stage / state,
   // barrier state, iteration), readable while the kernel runs; else nullptr
   volatile int32_t *progress;
-  unsigned long long *arrive_groups;  // hot barriers: per-group arrival counters, then release words [2G * kArriveStride]
+  unsigned long long *arrive_groups;  // hot barriers: per-group arrival counters [G * kArriveStride]
   Params P;
 };
 
