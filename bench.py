@@ -408,6 +408,45 @@ def run_profile_case(args) -> None:
     print(json.dumps(out), flush=True)
 
 
+def spmv_bytes(rows, cols, nnz, word):
+    """Compulsory bytes of one SpMV: each nonzero's index and value, the row
+    pointers, the input vector once and the output vector."""
+    return nnz * (word + 4) + 4 * (rows + 1) + word * cols + word * rows
+
+
+def run_spmv_case(args) -> None:
+    """The seam's Kernels.spmv on the bench workload's equilibration-free K
+    (m x n) and its transpose, in both precisions: --spmv-reps calls each,
+    back to back on the context's stream, timed from the host around the
+    whole run (launch-bound when a call is shorter than its submission).  For
+    device-side times run it under ncu's launch list; the line gives each
+    matrix's compulsory bytes to divide by them."""
+    from noaidi_b200.prima import cuda, generators as G
+    p = G.dc_lopf(seed=0, **WORKLOAD)
+    K = p.constraint_matrix
+    Kt = K.transpose
+    out = {"spmv_case": True, "reps": args.spmv_reps, "matrices": {}}
+    for prec in (32, 64):
+        k = cuda.CudaKernels(0, prec)
+        for name, A in (("K", K), ("Kt", Kt)):
+            dA = k.upload_matrix(A)
+            x = k.upload(np.random.default_rng(0).standard_normal(A.cols))
+            y = k.allocate(A.rows)
+            k.spmv(dA, x, y)
+            k.dot(y, y)  # synchronises
+            t = time.perf_counter()
+            for _ in range(args.spmv_reps):
+                k.spmv(dA, x, y)
+            k.dot(y, y)
+            secs = (time.perf_counter() - t) / args.spmv_reps
+            byts = spmv_bytes(A.rows, A.cols, A.nnz, prec // 8)
+            out["matrices"][f"{name}_fp{prec}"] = {"rows": A.rows, "cols": A.cols, "nnz": int(A.nnz),
+                                                   "bytes": byts, "host_us_per_call": secs * 1e6,
+                                                   "host_gbs": byts / secs / 1e9}
+        k.close()
+    print(json.dumps(out), flush=True)
+
+
 def run_fp64_study(args) -> None:
     """The FP32 refinement against plain FP64 device PDHG, both solved to
     --eps in full, on every seed of --fp64-study: times, iterations, statuses,
@@ -458,6 +497,8 @@ def main():
                          "'batch' (0: off)")
     ap.add_argument("--fp64-study", default="",
                     help="comma-separated seeds: only compare the refinement with plain FP64, both in full, per seed")
+    ap.add_argument("--spmv-reps", type=int, default=0,
+                    help="only time the seam SpMV on the workload's K and K' (this many calls each) and exit")
     ap.add_argument("--profile-iterations", type=int, default=0,
                     help="only run this many PDHG iterations of the workload (a bounded case for ncu) and exit")
     ap.add_argument("--profile-precision", type=int, default=32, choices=[32, 64])
@@ -470,6 +511,8 @@ def main():
         return run_reference(args)
     if args.profile_iterations:
         return run_profile_case(args)
+    if args.spmv_reps:
+        return run_spmv_case(args)
     if args.fp64_study:
         return run_fp64_study(args)
 

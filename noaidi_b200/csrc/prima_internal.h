@@ -55,7 +55,7 @@ struct Mat {
   int32_t rows = 0, cols = 0;
   int64_t nnz = 0;
   DeviceBuffer row_ptr, col_idx, vals;
-  int32_t lanes = 1;  // SpMV variant picked by the autotuner (1 = thread per row)
+  int32_t lanes = 0;  // SpMV kernel picked by the autotuner (0: CSR-stream tiles, 1: thread per row)
 };
 
 struct LpHostCopy;

@@ -192,27 +192,53 @@ __global__ void k_spmv_row(int32_t rows, const int32_t *__restrict__ rp, const i
   }
 }
 
-// CSR SpMV with LANES threads per row (a sub-warp): strided partial sums,
-// combined by shuffles.  Faster on long rows; the summation order is a
-// fixed tree, not the index order.  The row loop advances warp-uniformly so
-// every lane reaches every shuffle.
-template <typename T, int LANES>
-__global__ void k_spmv_vec(int32_t rows, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
-                           const T *__restrict__ v, const T *__restrict__ x, T *__restrict__ out) {
-  constexpr int kGroups = 32 / LANES;  // rows per warp per step
-  const int lane = threadIdx.x & 31;
-  const int sub = lane / LANES, sl = lane % LANES;
-  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t base = warp * kGroups; base < rows; base += nwarps * kGroups) {
-    const int64_t r = base + sub;
-    T acc = T(0);
-    if (r < rows) {
-      const int32_t e = rp[r + 1];
-      for (int32_t p = rp[r] + sl; p < e; p += LANES) acc = acc + (v[p] * x[ci[p]]);
+// CSR SpMV by row tiles (CSR-stream): a block takes kStreamRows consecutive
+// rows at a time; its threads first form the tile's products v[k] * x[col[k]]
+// (rounded to T) with coalesced index and value loads and every gather of
+// the tile in flight at once, into shared memory; then each thread sums its
+// rows' products in index order from zero -- the same sum, bit for bit, as
+// one thread per row, with the memory traffic of a streaming kernel.  A tile
+// whose nonzeros do not fit is summed straight from global memory, in the
+// same order.
+constexpr int kStreamRows = 512;   // rows per tile (two per thread)
+constexpr int kStreamCap = 4096;   // products a tile stages
+
+template <typename T>
+__global__ void __launch_bounds__(kOpThreads) k_spmv_stream(int32_t rows, const int32_t *__restrict__ rp,
+                                                            const int32_t *__restrict__ ci, const T *__restrict__ v,
+                                                            const T *__restrict__ x, T *__restrict__ out) {
+  __shared__ T prod[kStreamCap];
+  static_assert(kStreamRows == 2 * kOpThreads, "two rows per thread");
+  for (int64_t r0 = (int64_t)blockIdx.x * kStreamRows; r0 < rows; r0 += (int64_t)gridDim.x * kStreamRows) {
+    const int32_t r1 = (int32_t)min((int64_t)rows, r0 + kStreamRows);
+    const int32_t k0 = rp[r0], k1 = rp[r1];
+    int32_t ra[2], rb[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int64_t r = r0 + threadIdx.x + q * kOpThreads;
+      ra[q] = r < r1 ? rp[r] : 0;
+      rb[q] = r < r1 ? rp[r + 1] : 0;
     }
-    for (int o = LANES / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, LANES);
-    if (r < rows && sl == 0) out[r] = acc;
+    const bool staged = k1 - k0 <= kStreamCap;
+    if (staged) {
+#pragma unroll 4
+      for (int32_t k = k0 + threadIdx.x; k < k1; k += kOpThreads) prod[k - k0] = v[k] * x[ci[k]];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int64_t r = r0 + threadIdx.x + q * kOpThreads;
+      if (r < r1) {
+        T acc = T(0);
+        if (staged) {
+          for (int32_t k = ra[q]; k < rb[q]; k++) acc = acc + prod[k - k0];
+        } else {
+          for (int32_t k = ra[q]; k < rb[q]; k++) acc = acc + (v[k] * x[ci[k]]);
+        }
+        out[r] = acc;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -223,15 +249,12 @@ static void launch_spmv(const Ctx *c, const Mat *a, const T *x, T *out) {
   const int32_t *rp = (const int32_t *)a->row_ptr.ptr;
   const int32_t *ci = (const int32_t *)a->col_idx.ptr;
   const T *v = (const T *)a->vals.ptr;
-  const int64_t threads = (int64_t)rows * a->lanes;
-  const unsigned g = grid_for(threads, c);
-  switch (a->lanes) {
-    case 1: k_spmv_row<T><<<g, kOpThreads, 0, c->stream>>>(rows, rp, ci, v, x, out); break;
-    case 2: k_spmv_vec<T, 2><<<g, kOpThreads, 0, c->stream>>>(rows, rp, ci, v, x, out); break;
-    case 4: k_spmv_vec<T, 4><<<g, kOpThreads, 0, c->stream>>>(rows, rp, ci, v, x, out); break;
-    case 8: k_spmv_vec<T, 8><<<g, kOpThreads, 0, c->stream>>>(rows, rp, ci, v, x, out); break;
-    case 16: k_spmv_vec<T, 16><<<g, kOpThreads, 0, c->stream>>>(rows, rp, ci, v, x, out); break;
-    default: k_spmv_vec<T, 32><<<g, kOpThreads, 0, c->stream>>>(rows, rp, ci, v, x, out); break;
+  if (a->lanes == 0) {  // CSR-stream tiles
+    const int64_t tiles = ((int64_t)rows + kStreamRows - 1) / kStreamRows;
+    const unsigned g = (unsigned)std::min<int64_t>(tiles, (int64_t)c->num_sms * 8);
+    k_spmv_stream<T><<<g, kOpThreads, 0, c->stream>>>(rows, rp, ci, v, x, out);
+  } else {
+    k_spmv_row<T><<<grid_for(rows, c), kOpThreads, 0, c->stream>>>(rows, rp, ci, v, x, out);
   }
 }
 
@@ -242,40 +265,48 @@ int32_t seam_spmv(Ctx *c, const Mat *a, const void *x, void *out) {
   return PRIMA_OK;
 }
 
-// Autotuner for the seam SpMV: a 64-bit context keeps one thread per row so
-// every row is summed in the reference's index order; a 32-bit context times
-// the sub-warp widths on the uploaded matrix and keeps the fastest.
-static int32_t autotune_spmv(Ctx *c, Mat *a) {
-  a->lanes = 1;
-  if (c->bits == 64 || a->rows == 0 || a->nnz < (int64_t)1 << 16) return PRIMA_OK;
-  DeviceBuffer xb, ob;
-  int32_t rc;
-  if ((rc = xb.reserve((size_t)a->cols * 4 + 16)) || (rc = ob.reserve((size_t)a->rows * 4 + 16))) return rc;
-  PRIMA_CUDA_TRY(cudaMemsetAsync(xb.ptr, 0, (size_t)a->cols * 4, c->stream));
+// Autotuner for the seam SpMV: both kernels sum every row in the
+// reference's index order (bit-exact in either precision), so the choice is
+// by speed alone -- each is timed on the uploaded matrix (a few launches
+// between CUDA events) and the faster kept.
+template <typename T>
+static int32_t time_spmv(Ctx *c, Mat *a, const T *x, T *out, int variant, float *ms) {
+  a->lanes = variant;
+  launch_spmv<T>(c, a, x, out);  // warm-up
   cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  float best = 1e30f;
-  int best_lanes = 1;
-  const int cand[] = {1, 2, 4, 8, 16, 32};
-  for (int lanes : cand) {
-    a->lanes = lanes;
-    launch_spmv<float>(c, a, (const float *)xb.ptr, (float *)ob.ptr);  // warm-up
-    cudaEventRecord(e0, c->stream);
-    for (int rep = 0; rep < 5; rep++) launch_spmv<float>(c, a, (const float *)xb.ptr, (float *)ob.ptr);
-    cudaEventRecord(e1, c->stream);
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (ms < best) {
-      best = ms;
-      best_lanes = lanes;
-    }
-  }
+  PRIMA_CUDA_TRY(cudaEventCreate(&e0));
+  PRIMA_CUDA_TRY(cudaEventCreate(&e1));
+  cudaEventRecord(e0, c->stream);
+  for (int rep = 0; rep < 5; rep++) launch_spmv<T>(c, a, x, out);
+  cudaEventRecord(e1, c->stream);
+  cudaEventSynchronize(e1);
+  *ms = 0.f;
+  cudaEventElapsedTime(ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  a->lanes = best_lanes;
   PRIMA_CUDA_TRY(cudaGetLastError());
+  return PRIMA_OK;
+}
+
+static int32_t autotune_spmv(Ctx *c, Mat *a) {
+  a->lanes = 0;
+  if (a->rows == 0 || a->nnz < (int64_t)1 << 16) return PRIMA_OK;
+  const size_t es = c->bits == 64 ? 8 : 4;
+  DeviceBuffer xb, ob;
+  int32_t rc;
+  if ((rc = xb.reserve((size_t)a->cols * es + 16)) || (rc = ob.reserve((size_t)a->rows * es + 16))) return rc;
+  PRIMA_CUDA_TRY(cudaMemsetAsync(xb.ptr, 0, (size_t)a->cols * es, c->stream));
+  float t_stream = 0.f, t_row = 0.f;
+  if (c->bits == 64) {
+    if ((rc = time_spmv<double>(c, a, (const double *)xb.ptr, (double *)ob.ptr, 0, &t_stream)) ||
+        (rc = time_spmv<double>(c, a, (const double *)xb.ptr, (double *)ob.ptr, 1, &t_row)))
+      return rc;
+  } else {
+    if ((rc = time_spmv<float>(c, a, (const float *)xb.ptr, (float *)ob.ptr, 0, &t_stream)) ||
+        (rc = time_spmv<float>(c, a, (const float *)xb.ptr, (float *)ob.ptr, 1, &t_row)))
+      return rc;
+  }
+  a->lanes = t_row < t_stream ? 1 : 0;
   return PRIMA_OK;
 }
 

@@ -144,12 +144,9 @@ def test_random_parity_with_the_oracle_ops(precision, mode):
         dA = k.upload_matrix(A)
         out = k.allocate(rows)
         k.spmv(dA, k.upload(x), out)
-        exact_spmv = precision == 64
+        # every row summed in index order: bit-exact in both precisions
         got, want = down(k, out), ops.spmv(A, ux)
-        if exact_spmv:
-            assert np.array_equal(got, want)
-        else:
-            assert np.allclose(got, want, rtol=1e-5, atol=1e-5)
+        assert np.array_equal(got, want)
         o = k.allocate(cols)
         k.axpby(0.37, k.upload(x), -1.25, k.upload(kt), o)
         assert np.array_equal(down(k, o), ops.axpby(0.37, ux, -1.25, ops.upload(kt)))
@@ -165,3 +162,27 @@ def test_random_parity_with_the_oracle_ops(precision, mode):
         d = k.dot(k.upload(x), k.upload(kt))
         assert abs(d - float(np.dot(ux, ops.upload(kt)))) <= 1e-9 * np.abs(ux * ops.upload(kt)).sum()
         assert abs(k.squared_norm(k.upload(x)) - float(ux @ ux)) <= 1e-9 * float(ux @ ux)
+
+
+@pytest.mark.parametrize("mode,precision", [(O.FP64, 64), (O.FP32, 32)], ids=["fp64", "fp32"])
+def test_spmv_bit_exact_on_long_and_short_rows(mode, precision):
+    """A matrix whose rows range from empty to 12,000 nonzeros, large enough
+    that the seam's autotuner times both of its kernels: every row is the
+    reference's index-order sum, whichever kernel the tuner kept and whether
+    or not a row's tile fits the kernel's staging area."""
+    from noaidi_b200.prima.cuda import CudaKernels
+    rng = np.random.default_rng(11)
+    rows, cols = 20000, 15000
+    lengths = rng.integers(0, 9, rows)
+    lengths[[3, 777, 19999]] = [12000, 5000, 4097]
+    r = np.repeat(np.arange(rows), lengths)
+    c = np.concatenate([rng.choice(cols, size=k, replace=False) for k in lengths])
+    A = SparseMatrix.from_triplets(rows, cols, r, c, rng.standard_normal(len(r)))
+    ops = O.Ops(mode)
+    x = rng.standard_normal(cols)
+    with CudaKernels(0, precision) as k:
+        dA = k.upload_matrix(A)
+        out = k.allocate(rows)
+        for _ in range(2):  # twice: the second call reuses the same kernel choice
+            k.spmv(dA, k.upload(x), out)
+            assert np.array_equal(down(k, out), ops.spmv(A, ops.upload(x)))
