@@ -389,8 +389,10 @@ def run_profile_case(args) -> None:
     params = PdhgParams(eps_abs=eps, eps_rel=eps, max_iterations=args.profile_iterations)
     out = {"profile_case": True, "workload": args.profile_workload, "n": problem.num_variables,
            "m": problem.num_constraints, "nnz": problem.constraint_matrix.nnz, "build_s": build_s, "eps": eps}
+    ctx = cuda.Context(0, 32 if args.profile_mixed else args.profile_precision)
+    if args.profile_layout:
+        ctx.set_solver_layout(*[int(v) for v in args.profile_layout.split(",")])
     if args.profile_mixed:
-        ctx = cuda.Context(0, 32)
         resident = cuda.DeviceProblem(problem, params, ctx=ctx)
         r = resident.mixed_solve(params, MixedPrecisionParams(reduced_max_iterations=params.max_iterations),
                                  scheme=cuda.MIXED_REFINEMENT, round_reduction=args.round_reduction,
@@ -399,11 +401,11 @@ def run_profile_case(args) -> None:
         out.update(precision="fp32+fp64", reduced_iterations=r.reduced_iterations,
                    refinement_iterations=r.refinement_iterations)
     else:
-        resident = cuda.DeviceProblem(problem, params, precision=args.profile_precision)
+        resident = cuda.DeviceProblem(problem, params, ctx=ctx)
         s = resident.solve(params, want_solution=False)
         out.update(precision=args.profile_precision)
     out.update(status=s.status.name, objective=s.objective_value, iterations=s.iterations, trials=s.trials,
-               blocks=s.blocks, device_s=s.device_ms / 1e3, us_per_trial=1e3 * s.device_ms / max(1, s.trials))
+               blocks=s.blocks, tile_rows=s.tile_rows, device_s=s.device_ms / 1e3, us_per_trial=1e3 * s.device_ms / max(1, s.trials))
     resident.free()
     print(json.dumps(out), flush=True)
 
@@ -506,6 +508,8 @@ def main():
     ap.add_argument("--profile-workload", default="dc-lopf", choices=["dc-lopf", "sclopf-n1", "expansion-storage"])
     ap.add_argument("--profile-mixed", action="store_true")
     ap.add_argument("--profile-tolerance", type=float, default=EPS)
+    ap.add_argument("--profile-layout", default="",
+                    help="BLOCKS_PER_SM,TILE_ROWS: pin the solver's layout instead of choosing it by timing")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -623,7 +627,7 @@ def main():
                          "dual_residual": sol.kkt.dual_residual_norm, "gap": sol.kkt.absolute_gap,
                          "fp32_pass_iterations": last.reduced_iterations,
                          "refinement_iterations": last.refinement_iterations,
-                         "rounds": last.refinement_rounds, "blocks": sol.blocks,
+                         "rounds": last.refinement_rounds, "layout": {"blocks": sol.blocks, "tile_rows": sol.tile_rows},
                          "e2e_status": r_e2e.solution.status.name},
         }
         h = highs_reference(0, problem) if rank == 0 else None

@@ -78,6 +78,17 @@ int32_t prima_capabilities_get(prima_handle ctx, prima_capabilities *out);
  * a block's own bulk copies keep their fixed bound.  No counterpart in the
  * reference. */
 int32_t prima_set_device_wait_limit(prima_handle ctx, int64_t polls);
+/* The persistent solver's layout for problems of more than 4,096 rows or
+ * columns: blocks per SM and the row cap of the tiles its hot phases stream.
+ * By default (both 0) the layout is chosen per problem and precision the
+ * first time the problem is solved: a few candidates (the most blocks that
+ * fit or one fewer; full or half tiles) each run a short bounded solve, and
+ * the fastest per step-size trial is kept.  The layout decides how the team
+ * groups its sums, so it can move the last bits of a result; pinning one
+ * (blocks_per_sm > 0; tile_rows 512 or 256) makes results repeat exactly
+ * across runs.  No counterpart in the reference, whose solve runs on one
+ * thread. */
+int32_t prima_set_solver_layout(prima_handle ctx, int32_t blocks_per_sm, int32_t tile_rows);
 
 /* ---- memory (Kernels.scala:51-63) ---------------------------------------- */
 /* Kernels.allocate: a zero-filled vector of length n. */
@@ -197,8 +208,8 @@ typedef struct {
   double setup_ms;  /* scaling, transpose and upload */
   int64_t trials;   /* step-size trials, accepted and rejected */
   double span_ms;   /* CUDA-event time from the call's first device work to its last */
-  int32_t blocks;   /* blocks of the persistent kernel's team that ran the (last) pass */
-  int32_t pad2;
+  int32_t blocks;    /* blocks of the persistent kernel's team that ran the (last) pass */
+  int32_t tile_rows; /* row cap of that pass's hot-phase tiles (the solver layout) */
 } prima_solution_info;
 
 /* Pdhg.solveWith(problem, params, this-context, cancelled, warmStart).

@@ -79,8 +79,19 @@ struct PreparedLp {
   double scaled_c_norm = 0, scaled_q_norm = 0;
   std::vector<double> h_sc, h_sq, h_sl, h_su, h_cs, h_rs;  // host copies for warm starts
   std::vector<int32_t> h_kp, h_tp;                       // row pointers of K and K'
-  DeviceBuffer b_tiles[2][2];                            // [precision][K, K'] warp-tile tables (int2)
-  int32_t ntiles[2][2] = {{0, 0}, {0, 0}};
+  // hot-phase tiles per [precision][row cap: 512, 256][K, K']: the host
+  // table (first row, first nonzero; closed by rows, nnz), each tile's cost
+  // estimate, and on the device the tiles as (start, end) pairs in the order
+  // that hands them to a team of tiles_nb blocks (slot rank + k*nb is block
+  // rank's k-th tile)
+  std::vector<int2> h_tiles[2][2][2];
+  std::vector<float> h_tile_cost[2][2][2];
+  DeviceBuffer b_tiles[2][2][2];
+  int32_t ntiles[2][2][2] = {};
+  int32_t tiles_nb[2][2] = {};
+  // the solver layout chosen for this problem per precision (0: not yet):
+  // blocks per SM, and the tile table's row cap (index into b_tiles)
+  int32_t layout_bps[2] = {0, 0}, layout_rows[2] = {0, 0};
   std::unique_ptr<LpHostCopy> owned;  // the caller's problem, when held by a handle
   const prima_lp *host = nullptr;     // the caller's problem (valid while in use)
 
@@ -140,6 +151,7 @@ struct Ctx {
   int32_t *cancel_mapped = nullptr;  // pinned + mapped: cancel flag seen by the device
   int32_t *cancel_mapped_dev = nullptr;
   int64_t wait_limit = 0;      // team-barrier polls before a block gives up (0: the default)
+  int32_t pin_bps = 0, pin_rows = 0;  // a solver layout the caller pinned (0: chosen by timing)
   DeviceBuffer solver_arena;   // buffers of the coarse solvers, reused across solves
   DeviceBuffer batch_arena;    // state, arguments and queue of a batch launch
   PreparedLp scratch_lp;       // the problem of a one-shot solve call

@@ -415,6 +415,22 @@ extern "C" int32_t prima_set_device_wait_limit(prima_handle h, int64_t polls) {
   return PRIMA_OK;
 }
 
+extern "C" int32_t prima_set_solver_layout(prima_handle h, int32_t blocks_per_sm, int32_t tile_rows) {
+  clear_error();
+  int32_t rc;
+  Ctx *c = lookup_ctx(h, &rc);
+  if (!c) return rc;
+  if (blocks_per_sm < 0 || (blocks_per_sm > 0 && tile_rows != 512 && tile_rows != 256) ||
+      (blocks_per_sm == 0 && tile_rows != 0)) {
+    set_error("requirement failed: a pinned layout is blocks_per_sm > 0 with tile_rows 512 or 256; (0, 0) "
+              "restores the choice by timing");
+    return PRIMA_ERR_INVALID_ARGUMENT;
+  }
+  c->pin_bps = blocks_per_sm;
+  c->pin_rows = tile_rows;
+  return PRIMA_OK;
+}
+
 // ---- memory ---------------------------------------------------------------
 #define CTX_OR_RETURN(h)        \
   clear_error();                \

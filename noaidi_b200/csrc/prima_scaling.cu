@@ -289,7 +289,16 @@ int32_t PreparedLp::prepare(const prima_lp *lp, const prima_params *p, cudaStrea
   h_kp.assign(lp->row_ptr, lp->row_ptr + m + 1);
   h_tp.resize((size_t)n + 1);
   PRIMA_CUDA_TRY(cudaMemcpyAsync(h_tp.data(), b_tp.ptr, ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost, s));
-  ntiles[0][0] = ntiles[0][1] = ntiles[1][0] = ntiles[1][1] = 0;
+  for (int w = 0; w < 2; w++)
+    for (int v = 0; v < 2; v++) {
+      tiles_nb[w][v] = 0;
+      for (int k = 0; k < 2; k++) {
+        ntiles[w][v][k] = 0;
+        h_tiles[w][v][k].clear();
+        h_tile_cost[w][v][k].clear();
+      }
+    }
+  layout_bps[0] = layout_bps[1] = layout_rows[0] = layout_rows[1] = 0;
   PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
   scaled_c_norm = norm2(h_sc.data(), n);
   scaled_q_norm = norm2(h_sq.data(), m);

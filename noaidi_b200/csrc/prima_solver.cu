@@ -8,7 +8,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <limits>
+#include <queue>
 #include <thread>
 
 #include <math_constants.h>
@@ -16,6 +18,15 @@
 #include "prima_internal.h"
 #include "prima_nvtx.h"
 #include "prima_solver.cuh"
+
+// Weights of the hot tiles' cost estimate (tile_cost); all-zero weights but
+// the first deal the tiles round-robin.
+#ifndef PRIMA_TILE_COST_TILE
+#define PRIMA_TILE_COST_TILE 1.0f
+#define PRIMA_TILE_COST_ROW 0.0f
+#define PRIMA_TILE_COST_NNZ 0.0f
+#define PRIMA_TILE_COST_SECTOR 0.0f
+#endif
 
 namespace prima {
 namespace dev {
@@ -138,8 +149,9 @@ struct None {};
 // Phases A and B cut the rows of K' (A) and K (B) into tiles of at most
 // kRows rows, starting at a multiple of 4, whose nonzeros (rounded out to
 // 16-byte granules) fit one stage -- a table built once per matrix on the
-// host.  Block `rank` of `nb` takes tiles rank, rank + nb, ..., so every
-// block gets an even sample of the matrix.  A tile's row pointers, column
+// host and dealt to the team's blocks by estimated cost: the device table
+// holds (start, end) pairs, slot rank + k*nb being block `rank`'s k-th
+// tile.  A tile's row pointers, column
 // indices, values and up to six vector slices arrive in one of kStages
 // shared-memory stages by one-dimensional bulk copies (cp.async.bulk,
 // completion on the stage's mbarrier).  Each warp then works on its own 32
@@ -337,7 +349,7 @@ __device__ __forceinline__ void prime_tiles(int32_t ntiles, int nb, int rank, co
   const int32_t mine = rank < ntiles ? (ntiles - rank + nb - 1) / nb : 0;
   if (mine == 0) return;
   const int nj = min(kHotBatch, mine);
-  for (int e = lane; e < 2 * nj; e += 32) hs.tiles[e] = __ldg(table + rank + (int64_t)(e >> 1) * nb + (e & 1));
+  for (int e = lane; e < 2 * nj; e += 32) hs.tiles[e] = __ldg(table + 2 * (rank + (int64_t)(e >> 1) * nb) + (e & 1));
   __syncwarp();
   if (lane == 0) {
     hs.listed = table;
@@ -356,7 +368,7 @@ __device__ __forceinline__ void list_tiles(int32_t ntiles, int nb, int rank, con
   const int lane = threadIdx.x & 31;
   const int32_t mine = rank < ntiles ? (ntiles - rank + nb - 1) / nb : 0;
   const int nj = min(kHotBatch, mine);
-  for (int e = lane; e < 2 * nj; e += 32) hs.tiles[e] = __ldg(table + rank + (int64_t)(e >> 1) * nb + (e & 1));
+  for (int e = lane; e < 2 * nj; e += 32) hs.tiles[e] = __ldg(table + 2 * (rank + (int64_t)(e >> 1) * nb) + (e & 1));
   __syncwarp();
   if (lane == 0) hs.listed = table;
   __syncwarp();
@@ -380,7 +392,7 @@ __device__ __forceinline__ bool hot_tiles(int32_t ntiles, int nb, int rank, cons
     if (!pre) {
       if (!(jb == 0 && hs.listed == table))  // the first batch may already be staged
         for (int e = threadIdx.x; e < 2 * nj; e += kThreads) {
-          const int64_t t = rank + (int64_t)(jb + (e >> 1)) * nb + (e & 1);
+          const int64_t t = 2 * (rank + (int64_t)(jb + (e >> 1)) * nb) + (e & 1);
           hs.tiles[e] = __ldg(table + t);
         }
       __syncthreads();  // every thread has read hs.listed
@@ -1912,7 +1924,7 @@ inline int team_blocks(int64_t n, int64_t m, int max_blocks) {
 // 4 rows that alone does not fit is a tile of its own, read unstaged.
 // Entries are (first row, first nonzero), closed by (rows, nnz).
 template <typename T>
-std::vector<int2> tile_table(const std::vector<int32_t> &rp) {
+std::vector<int2> tile_table(const std::vector<int32_t> &rp, int64_t max_rows) {
   const int64_t rows = (int64_t)rp.size() - 1, cap = dev::HotLayout<T>::kCap;
   std::vector<int2> table;
   table.reserve((size_t)(rows / 16 + 2));
@@ -1920,7 +1932,7 @@ std::vector<int2> tile_table(const std::vector<int32_t> &rp) {
   while (r < rows) {
     table.push_back(make_int2((int)r, rp[r]));
     int64_t e = r;
-    while (e < rows && e - r < dev::kHotRows<T>) {
+    while (e < rows && e - r < max_rows) {
       const int64_t e2 = std::min<int64_t>(rows, e + 4);
       if (e > r && (((int64_t)rp[e2] + 3) & ~3) - (rp[r] & ~3) > cap) break;
       e = e2;
@@ -1931,20 +1943,127 @@ std::vector<int2> tile_table(const std::vector<int32_t> &rp) {
   return table;
 }
 
-// Builds (once per prepared problem and precision) and uploads the tables.
+// The row caps of the two tile tables a problem keeps per precision: full
+// tiles (two rows per thread) and half tiles.
+constexpr int kTableRows[2] = {dev::kHotRows<float> == dev::kHotRows<double> ? dev::kHotRows<float> : 0,
+                               dev::kHotRows<float> / 2};
+static_assert(kTableRows[0] > 0, "both precisions cut tiles of the same rows");
+
+// Estimated time of one hot tile, from its rows, its nonzeros and the
+// distinct 32-byte sectors its gathers touch (a gather's cost is the sector
+// it fetches, and a tile's rows share sectors when their indices are close).
+// The weights are a least-squares fit of blocks' measured work per trial on
+// config-2-sized LPs; only their ratios matter.
+inline float tile_cost(int64_t rows, int64_t nnz, int64_t sectors) {
+  constexpr float kTile = PRIMA_TILE_COST_TILE, kRow = PRIMA_TILE_COST_ROW, kNnz = PRIMA_TILE_COST_NNZ,
+                  kSector = PRIMA_TILE_COST_SECTOR;
+  return kTile + kRow * (float)rows + kNnz * (float)nnz + kSector * (float)sectors;
+}
+
+// The cost of every tile of table t over a matrix with row pointers rp and
+// column indices ci, gathering a vector of `cols` words of `word` bytes.
+// A marker per sector, stamped with the tile's number, counts each sector
+// once per tile.
+std::vector<float> tile_costs(const std::vector<int2> &t, const int32_t *rp, const int32_t *ci, int64_t cols,
+                              int word) {
+  const int shift = word == 8 ? 2 : 3;  // words per 32-byte sector: 4 or 8
+  const int64_t nt = (int64_t)t.size() - 1;
+  std::vector<int32_t> mark((size_t)((cols >> shift) + 1), -1);
+  std::vector<float> cost((size_t)std::max<int64_t>(nt, 0));
+  for (int64_t j = 0; j < nt; j++) {
+    int64_t sectors = 0;
+    for (int64_t k = rp[t[j].x]; k < rp[t[j + 1].x]; k++) {
+      int32_t &mk = mark[(size_t)(ci[k] >> shift)];
+      if (mk != (int32_t)j) mk = (int32_t)j, sectors++;
+    }
+    cost[j] = tile_cost(t[j + 1].x - t[j].x, (int64_t)rp[t[j + 1].x] - rp[t[j].x], sectors);
+  }
+  return cost;
+}
+
+// The tiles of table t handed to a team of nb blocks as (start, end) pairs,
+// slot rank + k*nb holding block rank's k-th tile.  Every block keeps the
+// tile count of a round-robin deal (the first ntiles mod nb blocks one
+// more), and the tiles go out heaviest first, each to the least-loaded
+// block that still has room (ties to the lower block); a block then runs
+// its tiles in table order.  The deal depends only on the table, the
+// costs and nb, so a problem's sums group the same way on every run.
+std::vector<int2> deal_tiles(const std::vector<int2> &t, const std::vector<float> &cost, int nb) {
+  const int64_t nt = (int64_t)t.size() - 1;
+  std::vector<int2> pairs((size_t)(2 * std::max<int64_t>(nt, 0)));
+  std::vector<int64_t> slot_tile((size_t)std::max<int64_t>(nt, 0));
+  if (nb <= 1 || nt <= nb) {
+    for (int64_t j = 0; j < nt; j++) slot_tile[j] = j;
+  } else {
+    std::vector<int64_t> order((size_t)nt);
+    for (int64_t j = 0; j < nt; j++) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return cost[x] > cost[y]; });
+    std::vector<int64_t> room((size_t)nb);
+    for (int b = 0; b < nb; b++) room[b] = nt / nb + (b < nt % nb ? 1 : 0);
+    using Load = std::pair<double, int>;
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (int b = 0; b < nb; b++) heap.push({0.0, b});
+    std::vector<std::vector<int64_t>> mine((size_t)nb);
+    for (int64_t j : order) {
+      const Load top = heap.top();
+      heap.pop();
+      mine[top.second].push_back(j);
+      if (--room[top.second] > 0) heap.push({top.first + (double)cost[j], top.second});
+    }
+    for (int b = 0; b < nb; b++) {
+      std::sort(mine[b].begin(), mine[b].end());
+      for (size_t k = 0; k < mine[b].size(); k++) slot_tile[(size_t)b + k * (size_t)nb] = mine[b][k];
+    }
+  }
+  for (int64_t s = 0; s < nt; s++) {
+    pairs[2 * s] = t[slot_tile[s]];
+    pairs[2 * s + 1] = t[slot_tile[s] + 1];
+  }
+  return pairs;
+}
+
+// Builds (once per prepared problem and precision) both tile tables of K
+// and K' with every tile's cost; the device copies are dealt per team size
+// by ensure_deal.
 template <typename T>
 int32_t ensure_tile_tables(PreparedLp &L, cudaStream_t s) {
   const int w = sizeof(T) == 8;
-  if (L.ntiles[w][0] || (L.m == 0 && L.n == 0)) return PRIMA_OK;
-  const std::vector<int32_t> *rps[2] = {&L.h_kp, &L.h_tp};
-  for (int k = 0; k < 2; k++) {
-    const std::vector<int2> t = tile_table<T>(*rps[k]);
-    int32_t rc;
-    if ((rc = L.b_tiles[w][k].reserve(t.size() * sizeof(int2)))) return rc;
-    PRIMA_CUDA_TRY(cudaMemcpyAsync(L.b_tiles[w][k].ptr, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+  if (L.ntiles[w][0][0] || L.ntiles[w][0][1] || (L.m == 0 && L.n == 0)) return PRIMA_OK;
+  std::vector<int32_t> kci((size_t)L.nnz), tci((size_t)L.nnz);
+  if (L.nnz) {
+    PRIMA_CUDA_TRY(cudaMemcpyAsync(kci.data(), L.kci(), (size_t)L.nnz * 4, cudaMemcpyDeviceToHost, s));
+    PRIMA_CUDA_TRY(cudaMemcpyAsync(tci.data(), L.tci(), (size_t)L.nnz * 4, cudaMemcpyDeviceToHost, s));
     PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
-    L.ntiles[w][k] = (int32_t)t.size() - 1;
   }
+  const std::vector<int32_t> *rps[2] = {&L.h_kp, &L.h_tp};
+  const int32_t *cis[2] = {kci.data(), tci.data()};
+  const int64_t cols[2] = {L.n, L.m};
+  for (int v = 0; v < 2; v++) {
+    L.tiles_nb[w][v] = 0;
+    for (int k = 0; k < 2; k++) {
+      L.h_tiles[w][v][k] = tile_table<T>(*rps[k], kTableRows[v]);
+      L.h_tile_cost[w][v][k] = tile_costs(L.h_tiles[w][v][k], rps[k]->data(), cis[k], cols[k], (int)sizeof(T));
+      L.ntiles[w][v][k] = (int32_t)L.h_tiles[w][v][k].size() - 1;
+    }
+  }
+  return PRIMA_OK;
+}
+
+// The device copies of tile table v dealt to a team of nb blocks.
+template <typename T>
+int32_t ensure_deal(PreparedLp &L, int v, int nb, cudaStream_t s) {
+  const int w = sizeof(T) == 8;
+  if (L.tiles_nb[w][v] == nb) return PRIMA_OK;
+  for (int k = 0; k < 2; k++) {
+    const std::vector<int2> pairs = deal_tiles(L.h_tiles[w][v][k], L.h_tile_cost[w][v][k], nb);
+    int32_t rc;
+    if ((rc = L.b_tiles[w][v][k].reserve(std::max<size_t>(1, pairs.size()) * sizeof(int2)))) return rc;
+    if (!pairs.empty())
+      PRIMA_CUDA_TRY(cudaMemcpyAsync(L.b_tiles[w][v][k].ptr, pairs.data(), pairs.size() * sizeof(int2),
+                                     cudaMemcpyHostToDevice, s));
+  }
+  PRIMA_CUDA_TRY(cudaStreamSynchronize(s));
+  L.tiles_nb[w][v] = nb;
   return PRIMA_OK;
 }
 
@@ -1964,6 +2083,7 @@ struct SolveRequest {
   bool anchored = false;    // iterate on the residual problem around an FP64 anchor
   double round_rho = 0.0;   // anchored: error reduction that opens a new round (0: never)
   int32_t *rounds = nullptr;
+  int table = 0;            // hot-phase tile table: 0 full tiles, 1 half tiles
 };
 
 int32_t check_warm(const PreparedLp &L, const prima_warm_start *w) {
@@ -2040,6 +2160,11 @@ int32_t setup_job(Ctx *c, Job<T> &j, char *base, const StateLayout<T> &S, int bl
   cudaStream_t s = c->stream;
   const int32_t n = L.n, m = L.m, neq = L.neq;
   const bool anchored = req.anchored;
+
+  if (L.n || L.m) {
+    const int32_t rc = ensure_deal<T>(L, req.table, blocks, s);
+    if (rc) return rc;
+  }
 
   const double bound = L.scaled_spectral_bound;
   double step = bound > 0.0 ? 1.0 / bound : 1.0;
@@ -2120,10 +2245,11 @@ int32_t setup_job(Ctx *c, Job<T> &j, char *base, const StateLayout<T> &S, int bl
   a.ctl = (dev::Control *)(base + S.ctl);
   a.sync = (dev::Sync *)(base + S.sync);
   a.prof = phase_times() ? (dev::Prof *)(base + S.prof) : nullptr;
-  a.tiles_k = (const int2 *)L.b_tiles[w][0].ptr;
-  a.tiles_t = (const int2 *)L.b_tiles[w][1].ptr;
-  a.ntiles_k = L.ntiles[w][0];
-  a.ntiles_t = L.ntiles[w][1];
+  const int tv = j.req.table;  // tile table: full or half tiles
+  a.tiles_k = (const int2 *)L.b_tiles[w][tv][0].ptr;
+  a.tiles_t = (const int2 *)L.b_tiles[w][tv][1].ptr;
+  a.ntiles_k = L.ntiles[w][tv][0];
+  a.ntiles_t = L.ntiles[w][tv][1];
 
   if (anchored) {
     a.anchored = 1;
@@ -2224,6 +2350,7 @@ int32_t finish_job(Ctx * /*c*/, Job<T> &j, float kms, int blocks) {
   info->trials = ctl.total_trials;
   info->solve_ms = (int64_t)ms_since(j.t0);
   info->blocks = blocks;
+  info->tile_rows = kTableRows[req.table];
   if (req.rounds) *req.rounds = ctl.rounds;
   if (a.prof) {
     dev::Prof prof;
@@ -2293,6 +2420,23 @@ int32_t finish_job(Ctx * /*c*/, Job<T> &j, float kms, int blocks) {
       for (int g = 0; g < 32; g++)
         if (nby[g]) std::fprintf(stderr, " %.1f", by[g] / nby[g]);
       std::fprintf(stderr, "\n");
+    }
+  }
+  if (a.prof && std::getenv("PRIMA_PHASE_TIMES_CSV")) {
+    // the per-block record as a table, one row per block, times in us per trial
+    dev::Prof prof;
+    PRIMA_CUDA_TRY(cudaMemcpy(&prof, a.prof, sizeof(prof), cudaMemcpyDeviceToHost));
+    if (FILE *f = std::fopen(std::getenv("PRIMA_PHASE_TIMES_CSV"), "w")) {
+      const double ca = (double)std::max<int64_t>(1, prof.phase_count[dev::PH_A]);
+      const double cb = (double)std::max<int64_t>(1, prof.phase_count[dev::PH_B]);
+      std::fprintf(f, "block,sm,work_a,work_b,wait_a,wait_b,arrive_a,arrive_b,decide\n");
+      for (int b = 0; b < std::min(blocks, dev::kProfBlocks); b++)
+        std::fprintf(f, "%d,%d,%.4f,%.4f,%.4f,%.4f,%.4f,%.4f,%.4f\n", b, prof.block_sm[b],
+                     1e-3 * (double)prof.block_work[0][b] / ca, 1e-3 * (double)prof.block_work[1][b] / cb,
+                     1e-3 * (double)prof.block_wait[0][b] / ca, 1e-3 * (double)prof.block_wait[1][b] / cb,
+                     1e-3 * (double)prof.block_arrive[0][b] / ca, 1e-3 * (double)prof.block_arrive[1][b] / cb,
+                     1e-3 * (double)prof.block_decide[b] / cb);
+      std::fclose(f);
     }
   }
   if (ctl.error) {
@@ -2372,7 +2516,79 @@ int32_t launch_timed(Ctx *c, const void *kernel, int blocks, void **kargs, const
 // Pdhg.Solve on a prepared problem: the host prologue, then the whole
 // iteration in one cooperative launch.
 template <typename T>
+int32_t solve_with_layout(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::time_point t_start, int bps,
+                          int table);
+
+// The solver layout for a multi-block problem: blocks per SM (the most that
+// fit, or one fewer: fewer blocks, more tiles each) and the tile table (full
+// or half tiles).  Unless the context pins one, each candidate runs a short
+// bounded solve of this problem (no outputs) and the fastest per step-size
+// trial is kept for the problem and precision; another candidate must beat
+// the first (the most blocks, full tiles) by 5 % to be chosen, so that timing
+// noise between close candidates does not change the layout, and with it the
+// grouping of the team's sums, from run to run.
+template <typename T>
+int32_t choose_layout(Ctx *c, PreparedLp &L, const SolveRequest &req, int per_sm, int *bps, int *table) {
+  const int w = sizeof(T) == 8;
+  if (c->pin_bps > 0) {
+    *bps = std::min(c->pin_bps, per_sm);
+    *table = c->pin_rows > 0 && c->pin_rows <= kTableRows[1] ? 1 : 0;
+    return PRIMA_OK;
+  }
+  if (L.layout_bps[w] > 0) {
+    *bps = L.layout_bps[w];
+    *table = L.layout_rows[w];
+    return PRIMA_OK;
+  }
+  struct Cand {
+    int bps, table;
+  } cands[3] = {{per_sm, 0}, {per_sm - 1, 0}, {per_sm, 1}};
+  prima_params tp = *req.params;
+  tp.max_iterations = 96;
+  tp.time_limit_ms = -1.0;
+  double best = 0.0;
+  int pick = 0;
+  for (int k = 0; k < 3; k++) {
+    if (cands[k].bps < 1) continue;
+    prima_solution_info info;
+    SolveRequest tr{&tp, nullptr, nullptr, nullptr, nullptr, nullptr, &info};
+    int32_t rc = solve_with_layout<T>(c, L, tr, Clock::now(), cands[k].bps, cands[k].table);
+    if (rc) return rc;
+    const double per_trial = info.device_ms / (double)std::max<int64_t>(1, info.trials);
+    if (k == 0 || per_trial < best * 0.95) {
+      best = per_trial;
+      pick = k;
+    }
+  }
+  L.layout_bps[w] = cands[pick].bps;
+  L.layout_rows[w] = cands[pick].table;
+  *bps = cands[pick].bps;
+  *table = cands[pick].table;
+  return PRIMA_OK;
+}
+
+template <typename T>
 int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::time_point t_start) {
+  int32_t rc;
+  {
+    Job<T> j;
+    j.L = &L;
+    j.req = req;
+    if ((rc = prepare_job(c, j))) return rc;  // the tile tables the layouts need
+  }
+  int max_blocks = 0;
+  if ((rc = max_coresident_blocks<T>(c, &max_blocks))) return rc;
+  const int per_sm = max_blocks / c->num_sms;
+  int bps = per_sm, table = 0;
+  if (team_blocks(L.n, L.m, max_blocks) > 1 && (rc = choose_layout<T>(c, L, req, per_sm, &bps, &table))) return rc;
+  return solve_with_layout<T>(c, L, req, t_start, bps, table);
+}
+
+template <typename T>
+int32_t solve_with_layout(Ctx *c, PreparedLp &L, const SolveRequest &req_in, Clock::time_point t_start, int bps,
+                          int table) {
+  SolveRequest req = req_in;
+  req.table = table;
   Job<T> j;
   j.L = &L;
   j.req = req;
@@ -2381,6 +2597,7 @@ int32_t solve_on_device(Ctx *c, PreparedLp &L, const SolveRequest &req, Clock::t
   if ((rc = prepare_job(c, j))) return rc;
   int max_blocks = 0;
   if ((rc = max_coresident_blocks<T>(c, &max_blocks))) return rc;
+  max_blocks = std::min(max_blocks, bps * c->num_sms);
   const int blocks = team_blocks(L.n, L.m, max_blocks);
   const StateLayout<T> S(L.n, L.m, blocks, req.anchored);
   if ((rc = c->solver_arena.reserve(S.bytes))) return rc;
@@ -2452,7 +2669,7 @@ int32_t solve_batch_on_device(Ctx *c, std::vector<Job<T>> &jobs, const volatile 
   int largest_solo = 1;
   for (int i = 0; i < count; i++) {
     const PreparedLp &L = *jobs[i].L;
-    tiles[i] = (int64_t)L.ntiles[w][0] + L.ntiles[w][1];
+    tiles[i] = (int64_t)L.ntiles[w][0][0] + L.ntiles[w][0][1];
     size[i] = (int64_t)L.n + L.m + L.nnz;
     largest_solo = std::max(largest_solo, team_blocks(L.n, L.m, max_blocks));
   }

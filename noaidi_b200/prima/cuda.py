@@ -74,7 +74,7 @@ class CInfo(C.Structure):
                 ("dual_objective", C.c_double), ("primal_residual", C.c_double), ("dual_residual", C.c_double),
                 ("final_step_size", C.c_double), ("final_primal_weight", C.c_double), ("device_ms", C.c_double),
                 ("setup_ms", C.c_double), ("trials", C.c_int64), ("span_ms", C.c_double), ("blocks", C.c_int32),
-                ("pad2", C.c_int32)]
+                ("tile_rows", C.c_int32)]
 
 
 class CMixedParams(C.Structure):
@@ -113,6 +113,7 @@ SIGNATURES = {
     "prima_close": (C.c_int32, [_H]),
     "prima_capabilities_get": (C.c_int32, [_H, C.POINTER(Capabilities)]),
     "prima_set_device_wait_limit": (C.c_int32, [_H, C.c_int64]),
+    "prima_set_solver_layout": (C.c_int32, [_H, C.c_int32, C.c_int32]),
     "prima_vec_alloc": (C.c_int32, [_H, C.c_int64, _HP]),
     "prima_vec_upload": (C.c_int32, [_H, _DP, C.c_int64, _HP]),
     "prima_vec_download": (C.c_int32, [_H, _H, _DP, C.c_int64]),
@@ -254,6 +255,11 @@ class Context:
             _check(self.lib.prima_close(self.handle))
             self._closed = True
 
+    def set_solver_layout(self, blocks_per_sm: int = 0, tile_rows: int = 0) -> None:
+        """Pin the persistent solver's layout (``prima_set_solver_layout``);
+        (0, 0) restores the choice by timing."""
+        _check(self.lib.prima_set_solver_layout(self.handle, blocks_per_sm, tile_rows))
+
     def set_device_wait_limit(self, polls: int) -> None:
         """Team-barrier polls before a block of a solve gives up
         (``prima_set_device_wait_limit``); 0 restores the default."""
@@ -377,6 +383,7 @@ def _solution(info: CInfo, x, y, rc) -> LpSolution:
     sol.trials = info.trials
     sol.span_ms = info.span_ms
     sol.blocks = info.blocks
+    sol.tile_rows = info.tile_rows
     return sol
 
 

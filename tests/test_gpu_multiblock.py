@@ -175,3 +175,29 @@ def test_batch_of_multi_block_teams():
     for n, r in zip(names, res):
         assert r.solution.blocks >= MIN_BLOCKS and r.solution.status == SolveStatus.OPTIMAL
         assert rel(r.solution.objective_value, FIX[n]["oracle_fp64"]["objective"]) <= 1e-8
+
+
+def test_solver_layouts_reach_the_same_answer_and_repeat_exactly():
+    """The persistent solver's layout (blocks per SM, tile row cap) is chosen
+    per problem by timing, or pinned: every layout reaches the oracle's
+    answer, and a pinned layout repeats its result bit for bit."""
+    from noaidi_b200.prima import cuda
+    p, rec = case("lopf-300x24"), FIX["lopf-300x24"]
+    ctx = cuda.Context(0, 64)
+    try:
+        auto = cuda.solve(p, P9, ctx=ctx)
+        assert auto.blocks > 1 and auto.tile_rows in (512, 256)
+        for bps, rows in ((2, 512), (2, 256), (1, 512)):
+            ctx.set_solver_layout(bps, rows)
+            a = cuda.solve(p, P9, ctx=ctx)
+            b = cuda.solve(p, P9, ctx=ctx)
+            assert a.tile_rows == rows and a.blocks > 1
+            assert a.status == SolveStatus.OPTIMAL
+            assert rel(a.objective_value, rec["oracle_fp64"]["objective"]) <= 1e-8
+            assert (a.iterations, a.objective_value) == (b.iterations, b.objective_value)
+            np.testing.assert_array_equal(a.primal, b.primal)
+        with pytest.raises(ValueError):
+            ctx.set_solver_layout(3, 100)
+        ctx.set_solver_layout(0, 0)
+    finally:
+        ctx.close()
