@@ -19,13 +19,13 @@
 #include "prima_nvtx.h"
 #include "prima_solver.cuh"
 
-// Weights of the hot tiles' cost estimate (tile_cost); all-zero weights but
-// the first deal the tiles round-robin.
+// Weights of the hot tiles' cost estimate (tile_cost): the distinct sectors
+// a tile gathers.  All-zero weights but the first deal the tiles round-robin.
 #ifndef PRIMA_TILE_COST_TILE
-#define PRIMA_TILE_COST_TILE 1.0f
+#define PRIMA_TILE_COST_TILE 0.0f
 #define PRIMA_TILE_COST_ROW 0.0f
 #define PRIMA_TILE_COST_NNZ 0.0f
-#define PRIMA_TILE_COST_SECTOR 0.0f
+#define PRIMA_TILE_COST_SECTOR 1.0f
 #endif
 
 namespace prima {
@@ -55,6 +55,29 @@ __device__ __forceinline__ unsigned long long atom_add_acq_rel_u64(unsigned long
   asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
   return old;
 }
+// An increment with release semantics that returns nothing: the thread does
+// not wait for the round trip.
+__device__ __forceinline__ void red_add_release_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+// Waiting blocks poll the team's counter with relaxed loads and acquire once
+// when it completes (1), or poll with acquire loads (0).
+#ifndef PRIMA_POLL_RELAXED
+#define PRIMA_POLL_RELAXED 0
+#endif
+// The trial's two barriers count arrivals on the team's counter with one
+// fire-and-forget release increment per block (1), or in two levels -- a
+// group counter, then the group's last block on the team's -- with
+// round-trip atomics (0).
+#ifndef PRIMA_HOT_RED
+#define PRIMA_HOT_RED 1
+#endif
 // Phase A's first tiles are staged during the barrier after phase B on the
 // guess that the trial is accepted (see barrier_decide); 0 stages its tile
 // list only.
@@ -1512,17 +1535,19 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     return true;
   }
   if (phase == PH_A || phase == PH_B) {
-    // The trial's barriers.  Every block counts itself in on its group's
-    // arrival counter and the last of each group on the team's (neither is
-    // ever reset: the k-th barrier completes when the team's counter reads
-    // k * G), and waits for the whole team; after phase B every block then reduces the
+    // The trial's barriers.  Every block counts itself in on the team's
+    // arrival counter with a release increment it does not wait for (or, with
+    // PRIMA_HOT_RED 0, on its group's counter, the last of each group then on
+    // the team's); no counter is ever reset: the k-th barrier completes when
+    // the team's counter reads k * G (G the blocks, or the groups), and every
+    // block waits for the whole team.  After phase B every block then reduces the
     // trial's partials itself, in the same fixed order, and takes the same
     // step-size decision on its own copy of the Control record.  Nothing is
     // published and no block waits for a deciding block: the decision inputs
     // (partials, iteration counts, step, weight) are the same everywhere, and
     // the decision reads no clock and no flag.
     unsigned long long &s_ep = hot_epoch();
-    const int groups = tm.nb < kArriveGroups ? tm.nb : kArriveGroups;
+    const int groups = PRIMA_HOT_RED ? tm.nb : (tm.nb < kArriveGroups ? tm.nb : kArriveGroups);
     __syncthreads();
     if (threadIdx.x == 0) {
       const unsigned long long target = (s_ep + 1) * (unsigned long long)groups;
@@ -1541,16 +1566,21 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
         }
         block_clock()[1] = now;
       }
+      s_last = 0;
+#if PRIMA_HOT_RED
+      (void)target;
+      red_add_release_u64(&a.sync->arrive, 1ull);
+#else
       // count in on the group's counter; the group's last block counts the
       // group in on the team's
       const int g = tm.rank % groups;
       const unsigned long long gsize = (unsigned long long)((tm.nb - g + groups - 1) / groups);
       const unsigned long long gold = atom_add_acq_rel_u64(a.arrive_groups + (size_t)g * kArriveStride, 1ull);
-      s_last = 0;
       if (gold + 1 == (s_ep + 1) * gsize) {
         const unsigned long long old = atom_add_acq_rel_u64(&a.sync->arrive, 1ull);
         s_last = old + 1 == target;
       }
+#endif
       s_ok = 1;
     }
     __syncthreads();
@@ -1562,7 +1592,11 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
       const unsigned long long target = (s_ep + 1) * (unsigned long long)groups;
       if (!s_last) {
         long long spins = 0;
+#if PRIMA_POLL_RELAXED
+        while (ld_relaxed_u64(&a.sync->arrive) < target) {
+#else
         while (ld_acquire_u64(&a.sync->arrive) < target) {
+#endif
           if (*((volatile int32_t *)&a.sync->abort)) break;
           if (++spins > a.P.spin_limit) {
             atomicExch(&a.sync->abort, 1);
@@ -1572,6 +1606,9 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
           __nanosleep(PRIMA_POLL_SLEEP_NS);
 #endif
         }
+#if PRIMA_POLL_RELAXED
+        fence_acq_rel_gpu();  // the polls were relaxed: acquire once, on leaving
+#endif
       }
       if (*((volatile int32_t *)&a.sync->abort)) s_ok = 0;
       s_ep += 1;
@@ -1580,7 +1617,9 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
         if (tm.rank < kProfBlocks && block_clock()[1]) a.prof->block_wait[phase == PH_B][tm.rank] += now - block_clock()[1];
         block_clock()[0] = now;  // the next phase starts (after B: once decided)
       }
-      if (a.prof && s_last) {  // the last arrival stands for the release
+      // the last arrival (with one-level counting: rank 0 seeing the
+      // release) stands for the release
+      if (a.prof && (PRIMA_HOT_RED ? tm.rank == 0 : s_last)) {
         const uint64_t now = global_timer_ns(), tr = ldv(&a.prof->t_release);
         if (tr) {
           a.prof->phase_ns[phase & 7] += now - tr;
@@ -1952,8 +1991,9 @@ static_assert(kTableRows[0] > 0, "both precisions cut tiles of the same rows");
 // Estimated time of one hot tile, from its rows, its nonzeros and the
 // distinct 32-byte sectors its gathers touch (a gather's cost is the sector
 // it fetches, and a tile's rows share sectors when their indices are close).
-// The weights are a least-squares fit of blocks' measured work per trial on
-// config-2-sized LPs; only their ratios matter.
+// Only the weights' ratios matter.  On the 1.34M-column DC-LOPF, dealing by
+// sectors took the slowest block's mean work per phase from 22.6 to 21.2 us
+// (K') and 18.7 to 17.7 us (K), against dealing round-robin.
 inline float tile_cost(int64_t rows, int64_t nnz, int64_t sectors) {
   constexpr float kTile = PRIMA_TILE_COST_TILE, kRow = PRIMA_TILE_COST_ROW, kNnz = PRIMA_TILE_COST_NNZ,
                   kSector = PRIMA_TILE_COST_SECTOR;
