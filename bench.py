@@ -396,12 +396,12 @@ def run_profile_case(args) -> None:
         ctx.set_solver_layout(*[int(v) for v in args.profile_layout.split(",")])
     if args.profile_mixed:
         resident = cuda.DeviceProblem(problem, params, ctx=ctx)
+        scheme = cuda.MIXED_TWO_PASS if args.profile_scheme == "two-pass" else cuda.MIXED_REFINEMENT
         r = resident.mixed_solve(params, MixedPrecisionParams(reduced_max_iterations=params.max_iterations),
-                                 scheme=cuda.MIXED_REFINEMENT, round_reduction=args.round_reduction,
-                                 want_solution=False)
+                                 scheme=scheme, round_reduction=args.round_reduction, want_solution=False)
         s = r.solution
-        out.update(precision="fp32+fp64", reduced_iterations=r.reduced_iterations,
-                   refinement_iterations=r.refinement_iterations)
+        out.update(precision="fp32+fp64", scheme=args.profile_scheme, round_reduction=args.round_reduction,
+                   reduced_iterations=r.reduced_iterations, refinement_iterations=r.refinement_iterations)
     else:
         resident = cuda.DeviceProblem(problem, params, ctx=ctx)
         s = resident.solve(params, want_solution=False)
@@ -509,6 +509,9 @@ def main():
     ap.add_argument("--profile-snapshots", type=int, default=WORKLOAD["snapshots"])
     ap.add_argument("--profile-workload", default="dc-lopf", choices=["dc-lopf", "sclopf-n1", "expansion-storage"])
     ap.add_argument("--profile-mixed", action="store_true")
+    ap.add_argument("--profile-scheme", default="refinement", choices=["refinement", "two-pass"],
+                    help="with --profile-mixed: FP32 refinement around an FP64 anchor, or the reference's FP32 "
+                         "pass then FP64 finish")
     ap.add_argument("--profile-tolerance", type=float, default=EPS)
     ap.add_argument("--profile-layout", default="",
                     help="BLOCKS_PER_SM,TILE_ROWS: pin the solver's layout instead of choosing it by timing")
