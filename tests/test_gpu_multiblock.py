@@ -201,3 +201,24 @@ def test_solver_layouts_reach_the_same_answer_and_repeat_exactly():
         ctx.set_solver_layout(0, 0)
     finally:
         ctx.close()
+
+
+def test_pinned_layout_repeats_across_contexts():
+    """The tiles are dealt to the team's blocks from the matrix alone (each
+    tile's gather sectors), so a pinned layout gives the same bits on a fresh
+    context, where the problem is uploaded, equilibrated and dealt again."""
+    from noaidi_b200.prima import cuda
+    p = case("lopf-500x16")
+    runs = []
+    for _ in range(2):
+        ctx = cuda.Context(0, 32)
+        try:
+            ctx.set_solver_layout(3, 512)
+            runs.append(cuda.solve(p, P5, ctx=ctx))
+        finally:
+            ctx.close()
+    a, b = runs
+    assert a.blocks >= MIN_BLOCKS and a.status == SolveStatus.OPTIMAL
+    assert (a.iterations, a.objective_value) == (b.iterations, b.objective_value)
+    np.testing.assert_array_equal(a.primal, b.primal)
+    np.testing.assert_array_equal(a.dual, b.dual)
