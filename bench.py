@@ -55,7 +55,7 @@ WORKLOAD_NAME = "dc-lopf-2000bus-3000line-1000gen-168h (n=1,344,000 m=840,000 nn
 # Iterations the plain FP64 device PDHG needed to reach 1e-8 on the seed-0
 # instance in a full solve (the default run measures it again and reports the
 # count it saw); only the reference arm, which runs without a GPU, uses this.
-FP64_ITERATIONS_TO_TOLERANCE = 1_216_064
+FP64_ITERATIONS_TO_TOLERANCE = 1_104_256
 ROUND_REDUCTION = 10.0
 BATCH_EPS = 1e-6
 CONFIG1 = dict(m=400, n=600, per_column=5)
