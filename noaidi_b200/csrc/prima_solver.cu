@@ -84,6 +84,11 @@ __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_re
 #ifndef PRIMA_SPEC_A
 #define PRIMA_SPEC_A 1
 #endif
+// A block waiting at a trial's barrier reads the team's abort flag (and
+// counts against its poll limit) on every PRIMA_ABORT_EVERY-th poll.
+#ifndef PRIMA_ABORT_EVERY
+#define PRIMA_ABORT_EVERY 8
+#endif
 #ifndef PRIMA_POLL_SLEEP_NS
 #define PRIMA_POLL_SLEEP_NS 32
 #endif
@@ -1591,16 +1596,27 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
     } else if (threadIdx.x == 0) {
       const unsigned long long target = (s_ep + 1) * (unsigned long long)groups;
       if (!s_last) {
+        // A poll is one load; the abort flag and the poll limit are read
+        // every PRIMA_ABORT_EVERY polls only, and not at all once the team
+        // is in: a block that gave up after arriving is missed here, and
+        // the others meet its abort at the next barrier, which it never
+        // reaches.
         long long spins = 0;
 #if PRIMA_POLL_RELAXED
         while (ld_relaxed_u64(&a.sync->arrive) < target) {
 #else
         while (ld_acquire_u64(&a.sync->arrive) < target) {
 #endif
-          if (*((volatile int32_t *)&a.sync->abort)) break;
-          if (++spins > a.P.spin_limit) {
-            atomicExch(&a.sync->abort, 1);
-            break;
+          if (++spins % PRIMA_ABORT_EVERY == 0) {
+            if (*((volatile int32_t *)&a.sync->abort)) {
+              s_ok = 0;
+              break;
+            }
+            if (spins > a.P.spin_limit) {
+              atomicExch(&a.sync->abort, 1);
+              s_ok = 0;
+              break;
+            }
           }
 #if PRIMA_POLL_SLEEP_NS > 0
           __nanosleep(PRIMA_POLL_SLEEP_NS);
@@ -1609,8 +1625,9 @@ __device__ bool barrier_decide(const Args<T> &a, Control &snap, int phase, const
 #if PRIMA_POLL_RELAXED
         fence_acq_rel_gpu();  // the polls were relaxed: acquire once, on leaving
 #endif
+      } else if (*((volatile int32_t *)&a.sync->abort)) {
+        s_ok = 0;
       }
-      if (*((volatile int32_t *)&a.sync->abort)) s_ok = 0;
       s_ep += 1;
       if (a.prof) {
         const uint64_t now = global_timer_ns();
