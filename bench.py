@@ -24,7 +24,7 @@ error   the refinement's objective against that FP64 answer and against
 batch   (--batch K, 256 by default) the uneven sweep of K DC-LOPF instances,
         FP32 refinement to 1e-6, one launch per pass: LPs/s, its own
         roofline, a CPU estimate and errors against HiGHS on a sample.
-config1 the 600-column random sparse LP solved to 1e-6 by the device and by
+sparse_lp the 600-column random sparse LP solved to 1e-6 by the device and by
         the oracle on a host core, both measured in full.
 
 ``--impl reference`` times the CPU restatement of the reference FP64 PDHG
@@ -58,8 +58,8 @@ WORKLOAD_NAME = "dc-lopf-2000bus-3000line-1000gen-168h (n=1,344,000 m=840,000 nn
 FP64_ITERATIONS_TO_TOLERANCE = 1_104_256
 ROUND_REDUCTION = 10.0
 BATCH_EPS = 1e-6
-CONFIG1 = dict(m=400, n=600, per_column=5)
-CONFIG1_EPS = 1e-6
+SPARSE_LP = dict(m=400, n=600, per_column=5)
+SPARSE_LP_EPS = 1e-6
 # DRAM bytes (read + write) per step-size trial of pdhg_kernel<float> on this
 # workload: dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of
 # one plain FP32 launch of 96 trials on it, 14.34 GB / 96.  The refinement's
@@ -196,17 +196,17 @@ def cpu_sample(problem, iters: int, repeats: int = 1):
     return float(np.median(times)), s.iterations
 
 
-def config1_problem():
+def sparse_lp_problem():
     from noaidi_b200.prima import generators as G
-    return G.random_sparse_lp(seed=0, **CONFIG1)
+    return G.random_sparse_lp(seed=0, **SPARSE_LP)
 
 
-def config1_oracle():
+def sparse_lp_oracle():
     """The 600-column LP solved to 1e-6 by the oracle on one host core, in full."""
     from noaidi_b200.prima import PdhgParams
     from oracle import oracle as O
-    p = config1_problem()
-    params = PdhgParams(eps_abs=CONFIG1_EPS, eps_rel=CONFIG1_EPS, max_iterations=1_000_000)
+    p = sparse_lp_problem()
+    params = PdhgParams(eps_abs=SPARSE_LP_EPS, eps_rel=SPARSE_LP_EPS, max_iterations=1_000_000)
     O.solve(p, params.copy(max_iterations=64))  # warm the library
     t = time.perf_counter()
     s = O.solve(p, params)
@@ -227,7 +227,7 @@ def run_reference(args) -> None:
     iters = FP64_ITERATIONS_TO_TOLERANCE
     lps = 1.0 / (per_iter * iters)
     hi = host_info()
-    c1 = config1_oracle()
+    c1 = sparse_lp_oracle()
     line = {"impl": "reference", "metric": METRIC, "value": lps, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / lps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -240,8 +240,8 @@ def run_reference(args) -> None:
                                        f"device in FP64 to reach 1e-8 (a full run of that solve on the CPU would "
                                        f"take about {per_iter * iters / 3600:.1f} h)"},
             "e2e": {"value": lps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "config1_measured": {"workload": "random sparse LP m=400 n=600 (5 nonzeros per column), seed 0",
-                                 "eps": CONFIG1_EPS, "cores": 1, "time_to_tolerance_s": c1["seconds"],
+            "sparse_lp_measured": {"workload": "random sparse LP m=400 n=600 (5 nonzeros per column), seed 0",
+                                 "eps": SPARSE_LP_EPS, "cores": 1, "time_to_tolerance_s": c1["seconds"],
                                  "iterations": c1["iterations"], "status": c1["status"],
                                  "objective": c1["objective"], "lps_per_s": 1.0 / c1["seconds"]}}
     print(json.dumps(line), flush=True)
@@ -304,7 +304,7 @@ def batch_cpu_baseline(pool, specs, nnz, iterations, sample: int = 8):
 
 
 def run_batch(args, rank, world, dist, pool):
-    """Config 3: an uneven sweep of ``--batch`` DC-LOPF instances (buses
+    """The batch sweep: an uneven sweep of ``--batch`` DC-LOPF instances (buses
     U{100..2000}, snapshots U{24..168}, load scale U[0.6, 0.95], seeded), FP32
     refinement to 1e-6, each pass one launch for all of this rank's
     instances (host buffers in and out: upload, equilibration and download
@@ -335,7 +335,7 @@ def run_batch(args, rank, world, dist, pool):
     ctx.close()
     its = [r.reduced_iterations + r.refinement_iterations for r in res]
     statuses = sorted({r.solution.status.name for r in res})
-    out = {"workload": f"config 3: {args.batch} uneven DC-LOPF instances (buses U{{100..2000}}, snapshots "
+    out = {"workload": f"batch sweep: {args.batch} uneven DC-LOPF instances (buses U{{100..2000}}, snapshots "
                        f"U{{24..168}}), FP32 refinement to {BATCH_EPS:g}",
            "instances": args.batch, "lps_per_s": args.batch / float(agg[0]), "seconds": float(agg[0]),
            "wall_seconds": float(agg[1]), "statuses_rank0": statuses,
@@ -497,7 +497,7 @@ def main():
     ap.add_argument("--cpu-sample-iterations", type=int, default=128)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--batch", type=int, default=256,
-                    help="config 3: solve this many uneven LOPF instances to 1e-6 as batches and report LPs/s under "
+                    help="the batch sweep: solve this many uneven LOPF instances to 1e-6 as batches and report LPs/s under "
                          "'batch' (0: off)")
     ap.add_argument("--fp64-study", default="",
                     help="comma-separated seeds: only compare the refinement with plain FP64, both in full, per seed")
@@ -573,7 +573,7 @@ def main():
     # CPU legs on the host cores while the device runs the comparison solves
     cpu_jobs = {}
     if pool is not None and not args.skip_cpu:
-        cpu_jobs["config1"] = pool.apply_async(config1_oracle)
+        cpu_jobs["sparse_lp"] = pool.apply_async(sparse_lp_oracle)
 
     # end to end through the one-shot C ABI call with host buffers
     barrier()
@@ -599,9 +599,9 @@ def main():
         res64.free()
         ctx64.close()
 
-    # config 1 on the device: the 600-column LP to 1e-6, one-shot calls
-    c1p = config1_problem()
-    c1params = PdhgParams(eps_abs=CONFIG1_EPS, eps_rel=CONFIG1_EPS, max_iterations=1_000_000)
+    # the 600-column random sparse LP on the device to 1e-6, one-shot calls
+    c1p = sparse_lp_problem()
+    c1params = PdhgParams(eps_abs=SPARSE_LP_EPS, eps_rel=SPARSE_LP_EPS, max_iterations=1_000_000)
     cuda.mixed_solve(c1p, c1params, ctx=ctx32)  # warm
     t = time.perf_counter()
     c1_dev = cuda.mixed_solve(c1p, c1params, scheme=cuda.MIXED_REFINEMENT, ctx=ctx32)
@@ -658,9 +658,9 @@ def main():
                             "traffic": TRAFFIC_BYTES_PER_TRIAL * trials32 / len(results) if TRAFFIC_BYTES_PER_TRIAL else None,
                             "peak_source": pk_src,
                             "per_trial_bytes": byts / max(1, trials32), "kernel_ms": 1e3 * kern_s / steps}
-        c1 = cpu_jobs["config1"].get() if "config1" in cpu_jobs else None
-        line["config1"] = {"workload": "random sparse LP m=400 n=600 (5 nonzeros per column), seed 0",
-                           "eps": CONFIG1_EPS, "device_refinement_s": c1_dev_s,
+        c1 = cpu_jobs["sparse_lp"].get() if "sparse_lp" in cpu_jobs else None
+        line["sparse_lp"] = {"workload": "random sparse LP m=400 n=600 (5 nonzeros per column), seed 0",
+                           "eps": SPARSE_LP_EPS, "device_refinement_s": c1_dev_s,
                            "device_status": c1_dev.solution.status.name,
                            "device_iterations": [c1_dev.reduced_iterations, c1_dev.refinement_iterations],
                            "device_fp64_s": c1_64.solve_time_millis / 1e3, "device_fp64_iterations": c1_64.iterations,

@@ -166,7 +166,7 @@ def lodf_matrix(net: Network) -> tuple[np.ndarray, np.ndarray]:
 
 def sclopf_n1(seed: int = 0, buses: int = 500, lines: int = 750, generators: int = 300, snapshots: int = 24,
               outages: int = 200, load_scale: float = 0.7, voll: float = 1000.0) -> LpProblem:
-    """N-1 security-constrained DC-LOPF (config 4): ``dc_lopf`` on a
+    """N-1 security-constrained DC-LOPF: ``dc_lopf`` on a
     spanning tree plus chords, and for every snapshot, monitored line l and
     contingency o != l with a non-zero factor, the rating range
     ``-s_nom_l <= f_l + LODF[l, o] f_o <= s_nom_l`` -- the reference's

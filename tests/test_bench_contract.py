@@ -26,7 +26,7 @@ def test_reference_arm_prints_one_contract_line():
     assert (d["config"]["n"], d["config"]["m"], d["config"]["nnz"]) == (1_344_000, 840_000, 3_024_000)
     assert d["cpu_baseline"]["extrapolated"] is True and "EXTRAPOLATED" in d["cpu_baseline"]["sample"]
     assert d["cpu_baseline"]["host_cores"] >= 1
-    c1 = d["config1_measured"]
+    c1 = d["sparse_lp_measured"]
     assert c1["status"] == "OPTIMAL" and c1["time_to_tolerance_s"] > 0 and c1["iterations"] > 0
 
 

@@ -163,7 +163,7 @@ def test_lopf_matches_oracle(precision, eps):
     assert got.kkt.dual_residual_norm <= eps + eps * np.linalg.norm(P.objective)
 
 
-def test_config1_random_sparse_lp():
+def test_random_sparse_lp_600_columns():
     P = G.random_sparse_lp(0)
     p = PdhgParams(eps_abs=1e-6, eps_rel=1e-6, max_iterations=400_000)
     ref, got = O.solve(P, p), gpu_solve(P, p)

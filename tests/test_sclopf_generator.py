@@ -1,4 +1,4 @@
-"""The N-1 security-constrained generator (config 4, generators.sclopf_n1)
+"""The N-1 security-constrained generator (generators.sclopf_n1)
 on CPU: LODF against explicit post-outage power flows, and small instances
 solved by the oracle meet every security row."""
 import numpy as np
