@@ -62,9 +62,9 @@ SPARSE_LP = dict(m=400, n=600, per_column=5)
 SPARSE_LP_EPS = 1e-6
 # DRAM bytes (read + write) per step-size trial of pdhg_kernel<float> on this
 # workload: dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of
-# one plain FP32 launch of 96 trials on it, 14.34 GB / 96.  The refinement's
+# one plain FP32 solve of 200 trials on it, 29.69 GB / 200.  The refinement's
 # anchored trials also read the dual bound (m words, 3.4 MB more at most).
-TRAFFIC_BYTES_PER_TRIAL = 149.3e6
+TRAFFIC_BYTES_PER_TRIAL = 148.5e6
 
 
 def peaks():
