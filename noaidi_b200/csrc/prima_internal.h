@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "prima_cuda.h"
+#include "prima_tiles.h"
 
 namespace prima {
 
@@ -84,7 +85,7 @@ struct PreparedLp {
   // estimate, and on the device the tiles as (start, end) pairs in the order
   // that hands them to a team of tiles_nb blocks (slot rank + k*nb is block
   // rank's k-th tile)
-  std::vector<int2> h_tiles[2][2][2];
+  std::vector<TileEdge> h_tiles[2][2][2];
   std::vector<float> h_tile_cost[2][2][2];
   DeviceBuffer b_tiles[2][2][2];
   int32_t ntiles[2][2][2] = {};

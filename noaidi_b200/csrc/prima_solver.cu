@@ -8,9 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <functional>
 #include <limits>
-#include <queue>
 #include <thread>
 
 #include <math_constants.h>
@@ -19,14 +17,6 @@
 #include "prima_nvtx.h"
 #include "prima_solver.cuh"
 
-// Weights of the hot tiles' cost estimate (tile_cost): the distinct sectors
-// a tile gathers.  All-zero weights but the first deal the tiles round-robin.
-#ifndef PRIMA_TILE_COST_TILE
-#define PRIMA_TILE_COST_TILE 0.0f
-#define PRIMA_TILE_COST_ROW 0.0f
-#define PRIMA_TILE_COST_NNZ 0.0f
-#define PRIMA_TILE_COST_SECTOR 1.0f
-#endif
 
 namespace prima {
 namespace dev {
@@ -1974,110 +1964,11 @@ inline int team_blocks(int64_t n, int64_t m, int max_blocks) {
   return (int)std::min<int64_t>(max_blocks, (work + dev::kTileRows - 1) / dev::kTileRows);
 }
 
-// The tile table of a matrix with row pointers rp: tiles of at most
-// kHotRows rows, starting at multiples of 4, grown 4 rows at a time while
-// their nonzeros (rounded out to 16-byte granules) fit one stage.  A group of
-// 4 rows that alone does not fit is a tile of its own, read unstaged.
-// Entries are (first row, first nonzero), closed by (rows, nnz).
-template <typename T>
-std::vector<int2> tile_table(const std::vector<int32_t> &rp, int64_t max_rows) {
-  const int64_t rows = (int64_t)rp.size() - 1, cap = dev::HotLayout<T>::kCap;
-  std::vector<int2> table;
-  table.reserve((size_t)(rows / 16 + 2));
-  int64_t r = 0;
-  while (r < rows) {
-    table.push_back(make_int2((int)r, rp[r]));
-    int64_t e = r;
-    while (e < rows && e - r < max_rows) {
-      const int64_t e2 = std::min<int64_t>(rows, e + 4);
-      if (e > r && (((int64_t)rp[e2] + 3) & ~3) - (rp[r] & ~3) > cap) break;
-      e = e2;
-    }
-    r = e;
-  }
-  table.push_back(make_int2((int)rows, rp[rows]));
-  return table;
-}
-
 // The row caps of the two tile tables a problem keeps per precision: full
 // tiles (two rows per thread) and half tiles.
 constexpr int kTableRows[2] = {dev::kHotRows<float> == dev::kHotRows<double> ? dev::kHotRows<float> : 0,
                                dev::kHotRows<float> / 2};
 static_assert(kTableRows[0] > 0, "both precisions cut tiles of the same rows");
-
-// Estimated time of one hot tile, from its rows, its nonzeros and the
-// distinct 32-byte sectors its gathers touch (a gather's cost is the sector
-// it fetches, and a tile's rows share sectors when their indices are close).
-// Only the weights' ratios matter.  On the 1.34M-column DC-LOPF, dealing by
-// sectors took the slowest block's mean work per phase from 22.6 to 21.2 us
-// (K') and 18.7 to 17.7 us (K), against dealing round-robin.
-inline float tile_cost(int64_t rows, int64_t nnz, int64_t sectors) {
-  constexpr float kTile = PRIMA_TILE_COST_TILE, kRow = PRIMA_TILE_COST_ROW, kNnz = PRIMA_TILE_COST_NNZ,
-                  kSector = PRIMA_TILE_COST_SECTOR;
-  return kTile + kRow * (float)rows + kNnz * (float)nnz + kSector * (float)sectors;
-}
-
-// The cost of every tile of table t over a matrix with row pointers rp and
-// column indices ci, gathering a vector of `cols` words of `word` bytes.
-// A marker per sector, stamped with the tile's number, counts each sector
-// once per tile.
-std::vector<float> tile_costs(const std::vector<int2> &t, const int32_t *rp, const int32_t *ci, int64_t cols,
-                              int word) {
-  const int shift = word == 8 ? 2 : 3;  // words per 32-byte sector: 4 or 8
-  const int64_t nt = (int64_t)t.size() - 1;
-  std::vector<int32_t> mark((size_t)((cols >> shift) + 1), -1);
-  std::vector<float> cost((size_t)std::max<int64_t>(nt, 0));
-  for (int64_t j = 0; j < nt; j++) {
-    int64_t sectors = 0;
-    for (int64_t k = rp[t[j].x]; k < rp[t[j + 1].x]; k++) {
-      int32_t &mk = mark[(size_t)(ci[k] >> shift)];
-      if (mk != (int32_t)j) mk = (int32_t)j, sectors++;
-    }
-    cost[j] = tile_cost(t[j + 1].x - t[j].x, (int64_t)rp[t[j + 1].x] - rp[t[j].x], sectors);
-  }
-  return cost;
-}
-
-// The tiles of table t handed to a team of nb blocks as (start, end) pairs,
-// slot rank + k*nb holding block rank's k-th tile.  Every block keeps the
-// tile count of a round-robin deal (the first ntiles mod nb blocks one
-// more), and the tiles go out heaviest first, each to the least-loaded
-// block that still has room (ties to the lower block); a block then runs
-// its tiles in table order.  The deal depends only on the table, the
-// costs and nb, so a problem's sums group the same way on every run.
-std::vector<int2> deal_tiles(const std::vector<int2> &t, const std::vector<float> &cost, int nb) {
-  const int64_t nt = (int64_t)t.size() - 1;
-  std::vector<int2> pairs((size_t)(2 * std::max<int64_t>(nt, 0)));
-  std::vector<int64_t> slot_tile((size_t)std::max<int64_t>(nt, 0));
-  if (nb <= 1 || nt <= nb) {
-    for (int64_t j = 0; j < nt; j++) slot_tile[j] = j;
-  } else {
-    std::vector<int64_t> order((size_t)nt);
-    for (int64_t j = 0; j < nt; j++) order[j] = j;
-    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return cost[x] > cost[y]; });
-    std::vector<int64_t> room((size_t)nb);
-    for (int b = 0; b < nb; b++) room[b] = nt / nb + (b < nt % nb ? 1 : 0);
-    using Load = std::pair<double, int>;
-    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
-    for (int b = 0; b < nb; b++) heap.push({0.0, b});
-    std::vector<std::vector<int64_t>> mine((size_t)nb);
-    for (int64_t j : order) {
-      const Load top = heap.top();
-      heap.pop();
-      mine[top.second].push_back(j);
-      if (--room[top.second] > 0) heap.push({top.first + (double)cost[j], top.second});
-    }
-    for (int b = 0; b < nb; b++) {
-      std::sort(mine[b].begin(), mine[b].end());
-      for (size_t k = 0; k < mine[b].size(); k++) slot_tile[(size_t)b + k * (size_t)nb] = mine[b][k];
-    }
-  }
-  for (int64_t s = 0; s < nt; s++) {
-    pairs[2 * s] = t[slot_tile[s]];
-    pairs[2 * s + 1] = t[slot_tile[s] + 1];
-  }
-  return pairs;
-}
 
 // Builds (once per prepared problem and precision) both tile tables of K
 // and K' with every tile's cost; the device copies are dealt per team size
@@ -2098,7 +1989,8 @@ int32_t ensure_tile_tables(PreparedLp &L, cudaStream_t s) {
   for (int v = 0; v < 2; v++) {
     L.tiles_nb[w][v] = 0;
     for (int k = 0; k < 2; k++) {
-      L.h_tiles[w][v][k] = tile_table<T>(*rps[k], kTableRows[v]);
+      L.h_tiles[w][v][k] = tile_table(rps[k]->data(), (int64_t)rps[k]->size() - 1, dev::HotLayout<T>::kCap,
+                                      kTableRows[v]);
       L.h_tile_cost[w][v][k] = tile_costs(L.h_tiles[w][v][k], rps[k]->data(), cis[k], cols[k], (int)sizeof(T));
       L.ntiles[w][v][k] = (int32_t)L.h_tiles[w][v][k].size() - 1;
     }
@@ -2112,7 +2004,8 @@ int32_t ensure_deal(PreparedLp &L, int v, int nb, cudaStream_t s) {
   const int w = sizeof(T) == 8;
   if (L.tiles_nb[w][v] == nb) return PRIMA_OK;
   for (int k = 0; k < 2; k++) {
-    const std::vector<int2> pairs = deal_tiles(L.h_tiles[w][v][k], L.h_tile_cost[w][v][k], nb);
+    static_assert(sizeof(TileEdge) == sizeof(int2), "the device reads the table as int2");
+    const std::vector<TileEdge> pairs = deal_tiles(L.h_tiles[w][v][k], L.h_tile_cost[w][v][k], nb);
     int32_t rc;
     if ((rc = L.b_tiles[w][v][k].reserve(std::max<size_t>(1, pairs.size()) * sizeof(int2)))) return rc;
     if (!pairs.empty())
